@@ -1,0 +1,171 @@
+/*
+ * rbim_sm100.h - C ABI of the B200 (sm_100a) Swendsen-Wang engine for the 2D
+ * +-J random-bond Ising model.
+ *
+ * Every entry point takes plain device pointers owned by the caller, sizes and
+ * a CUDA stream (passed as void*, NULL = legacy default stream), returns an
+ * int status (RBIM_OK or a negative RBIM_ERR_* code; rbim_last_error() gives
+ * the message of the calling thread's last failure) and launches work
+ * asynchronously on that stream.  Hot entry points allocate nothing: scratch
+ * memory is passed in by the caller, sized by the *_workspace_bytes queries.
+ * Entry points are reentrant; calls on different streams with disjoint
+ * buffers may overlap.
+ *
+ * Data layout ("linear bit planes"): site n = x*L + y of an L x L periodic
+ * lattice (x slow, y fast; reference src/rbim/lattice.py:5-23) is bit n & 31 of
+ * word n >> 5, with no row padding.  A plane of one lattice takes
+ * rbim_plane_words(L) 32-bit words (ceil(L*L/32) rounded up to a multiple of
+ * 4 so that planes stay 16-byte aligned); bits past L*L are zero.
+ *   spin plane:     bit set <=> s = -1
+ *   coupling pair:  JH plane (bond 2n, (x,y)->(x+1,y)) followed by the JV
+ *                   plane (bond 2n+1, (x,y)->(x,y+1)); bit set <=> J = -1
+ * Occupation masks at the labelling seam are bytes in the reference bond
+ * order (2*L*L per lattice, bond 2n horizontal, 2n+1 vertical).
+ *
+ * Random numbers: Philox4x32-10 keyed by the chain key, counter
+ * {block, sweep_lo, sweep_hi, stream}; stream 0 bonds (bond k -> word k&3 of
+ * block k>>2), stream 1 cluster flips (root r -> bit r&127 of block r>>7),
+ * stream 2 hot-start spins (site n -> bit n&127 of block n>>7, sweep 0).
+ * A bond is occupied iff satisfied and its word < thr, where
+ * thr = floor((1 - exp(-2/T)) * 2^32) (0 <= thr <= 2^32).
+ */
+#ifndef RBIM_SM100_H
+#define RBIM_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBIM_ABI_VERSION 1
+
+enum {
+    RBIM_OK = 0,
+    RBIM_ERR_INVALID = -1,     /* bad argument (size, pointer, alignment) */
+    RBIM_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    RBIM_ERR_UNSUPPORTED = -3  /* size outside what this entry point handles */
+};
+
+/* Status-word bits written by the kernels (device int32, OR-ed). */
+enum {
+    RBIM_STATUS_FIND_CAP = 1,  /* a union-find walk exceeded its bound */
+    RBIM_STATUS_UNION_CAP = 2, /* a union retried beyond its bound */
+    RBIM_STATUS_BAD_CHAIN = 4  /* a chain descriptor was out of range */
+};
+
+/*
+ * One Markov chain: one disorder realization at one temperature, the unit of
+ * work of the reference's run_single_realization (src/rbim/simulation.py:148-242).
+ * All fields are 8 bytes; the struct is 96 bytes with no padding.
+ */
+typedef struct rbim_chain_t {
+    uint64_t key;          /* Philox key of the chain */
+    uint64_t thr;          /* activation threshold, see above */
+    int64_t spin_off;      /* word offset of the chain's spin plane in the spin pool (multiple of 4) */
+    int64_t coupling_off;  /* word offset of the chain's JH plane in the coupling pool (multiple of 4) */
+    int64_t acc_off;       /* accumulator row of the chain's bin 0 */
+    int64_t rec_off;       /* record row of the chain's measured sweep 0, or -1 for no records */
+    uint64_t sweep;        /* absolute sweep counter of the chain; advanced by the sweep calls */
+    int64_t n_therm;       /* sweeps 0 .. n_therm-1 are thermalisation (unmeasured) */
+    int64_t n_bins;        /* measured sweeps are n_therm .. n_therm + n_bins*sweeps_per_bin - 1 */
+    int64_t sweeps_per_bin;
+    int64_t L;             /* linear size, 3 <= L */
+    int64_t reserved;      /* must be 0 */
+} rbim_chain_t;
+
+/*
+ * Accumulators.  Row r of acc_int holds 12 int64 sums over the measured
+ * sweeps of one bin, row r of acc_f64 holds 2 double sums, in this order:
+ *   acc_int: E, E^2, M, |M|, M^2, S1, |M_C1|, S2, n_clusters, wrap_x, wrap_y, wrap_any
+ *   acc_f64: M^4, |M_C1|/S1
+ * (reference PRIMITIVES, src/rbim/simulation.py:56-71; per-bin means are the
+ * sums divided by sweeps_per_bin).  Sweep calls add into the rows, so the
+ * caller zeroes them before the first call.
+ * Records (optional): 8 int32 per measured sweep:
+ *   E, M, n_clusters, S1, |M_C1|, S2, wrap_x, wrap_y
+ * (reference SweepResult, src/rbim/swendsen_wang.py:24-53).
+ */
+#define RBIM_ACC_INT 12
+#define RBIM_ACC_F64 2
+#define RBIM_REC_LEN 8
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *rbim_last_error(void);
+
+/* RBIM_ABI_VERSION of the loaded library. */
+int rbim_abi_version(void);
+
+/* Words of one bit plane for linear size L (ceil(L*L/32) rounded up to 4). */
+int64_t rbim_plane_words(int64_t L);
+
+/* Largest L the resident (on-chip) engine accepts. */
+int rbim_resident_max_l(void);
+
+/*
+ * Initial spins of n_chains chains (reference initial_spins,
+ * src/rbim/swendsen_wang.py:56-78): hot != 0 draws Philox stream 2 of each
+ * chain's key, hot == 0 sets every spin to +1.  chains is a device array.
+ */
+int rbim_init_spins(const rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, int hot, void *stream);
+
+/*
+ * Bond activation of one lattice (reference activate_bonds,
+ * src/rbim/clusters.py:48-79, with the Philox stream in place of numpy's
+ * generator): writes 2*L*L occupation bytes in bond order.  couplings is the
+ * JH plane followed by the JV plane.  Runs the same activation code as the
+ * sweep engines; workspace: rbim_activate_workspace_bytes(L).
+ */
+size_t rbim_activate_workspace_bytes(int64_t L);
+int rbim_activate(int64_t L, const uint32_t *spins, const uint32_t *couplings, uint64_t key, uint64_t thr,
+                  uint64_t sweep, uint8_t *occ, void *workspace, size_t workspace_bytes, void *stream);
+
+/*
+ * Cluster labelling with exact wrapping of n_lattices frozen occupation masks
+ * of the same L (reference label_and_wrap, src/rbim/clusters.py:144-159 and
+ * src/rbim/_unionfind.py:91-136).  occ: n_lattices * 2*L*L bytes (nonzero =
+ * occupied).  labels: n_lattices * L*L int32, the canonical labels (clusters
+ * numbered in order of their smallest site).  n_clusters: n_lattices int32.
+ * wraps: n_lattices * 2 bytes (wrap_x, wrap_y).  status: device int32.
+ * Lattices with L <= rbim_resident_max_l() run on chip and need no workspace;
+ * larger ones use rbim_label_wrap_workspace_bytes(L) bytes of workspace.
+ */
+size_t rbim_label_wrap_workspace_bytes(int64_t L);
+int rbim_label_wrap(int64_t L, int n_lattices, const uint8_t *occ, int32_t *labels, int32_t *n_clusters,
+                    uint8_t *wraps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream);
+
+/*
+ * Batched resident sweeps: every chain of the device array `chains` advances
+ * by up to n_sweeps sweeps (fewer when it reaches the end of its run), with
+ * one lattice per CTA held in shared memory for the whole call, fed by a
+ * persistent work queue.  The chains may have different L (all <= l_max <=
+ * rbim_resident_max_l()).  This is the engine behind many calls of the
+ * reference's run_single_realization (src/rbim/simulation.py:196-242) and
+ * sw_sweep (src/rbim/swendsen_wang.py:103-172).  records may be NULL.
+ * threads: CTA size (0 = default).  workspace: rbim_batched_workspace_bytes()
+ * bytes (the work-queue counter).
+ */
+size_t rbim_batched_workspace_bytes(void);
+int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
+                        const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
+                        int n_sweeps, int threads, int32_t *status, void *workspace, size_t workspace_bytes,
+                        void *stream);
+
+/*
+ * Plain sweeps of one chain (device descriptor `chain`) through the
+ * global-memory engine: one lattice per launch sequence, any L >= 3, the
+ * drop-in for one run_single_realization task.  L must equal chain->L.  Same
+ * accumulator and record contract as rbim_sweeps_batched.  workspace:
+ * rbim_plain_workspace_bytes(L).
+ */
+size_t rbim_plain_workspace_bytes(int64_t L);
+int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool, int64_t *acc_int,
+                      double *acc_f64, int32_t *records, int n_sweeps, int32_t *status, void *workspace,
+                      size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBIM_SM100_H */

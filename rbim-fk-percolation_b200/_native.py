@@ -1,0 +1,144 @@
+"""ctypes binding of ``librbim_sm100.so``, the C ABI declared in ``include/rbim_sm100.h``.
+
+There is no CPU fallback: every compute entry point goes through this library
+and raises if it is missing or if no CUDA device is present.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = [
+    "RbimError",
+    "lib",
+    "check",
+    "CHAIN_DTYPE",
+    "ACC_INT",
+    "ACC_F64",
+    "REC_LEN",
+    "plane_words",
+    "resident_max_l",
+    "EXPORTED_SYMBOLS",
+]
+
+ACC_INT = 12
+ACC_F64 = 2
+REC_LEN = 8
+
+#: numpy mirror of ``rbim_chain_t`` (96 bytes, every field 8 bytes).
+CHAIN_DTYPE = np.dtype(
+    [
+        ("key", "<u8"),
+        ("thr", "<u8"),
+        ("spin_off", "<i8"),
+        ("coupling_off", "<i8"),
+        ("acc_off", "<i8"),
+        ("rec_off", "<i8"),
+        ("sweep", "<u8"),
+        ("n_therm", "<i8"),
+        ("n_bins", "<i8"),
+        ("sweeps_per_bin", "<i8"),
+        ("L", "<i8"),
+        ("reserved", "<i8"),
+    ]
+)
+assert CHAIN_DTYPE.itemsize == 96
+
+#: Every function ``include/rbim_sm100.h`` declares.
+EXPORTED_SYMBOLS = (
+    "rbim_last_error",
+    "rbim_abi_version",
+    "rbim_plane_words",
+    "rbim_resident_max_l",
+    "rbim_init_spins",
+    "rbim_activate_workspace_bytes",
+    "rbim_activate",
+    "rbim_label_wrap_workspace_bytes",
+    "rbim_label_wrap",
+    "rbim_batched_workspace_bytes",
+    "rbim_sweeps_batched",
+    "rbim_plain_workspace_bytes",
+    "rbim_sweeps_plain",
+)
+
+
+class RbimError(RuntimeError):
+    """A call into the CUDA engine failed."""
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(l):
+    c_int, c_i64, c_u64, c_size, p = ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_void_p
+    l.rbim_last_error.restype = ctypes.c_char_p
+    l.rbim_last_error.argtypes = []
+    l.rbim_abi_version.restype = c_int
+    l.rbim_abi_version.argtypes = []
+    l.rbim_plane_words.restype = c_i64
+    l.rbim_plane_words.argtypes = [c_i64]
+    l.rbim_resident_max_l.restype = c_int
+    l.rbim_resident_max_l.argtypes = []
+    l.rbim_init_spins.restype = c_int
+    l.rbim_init_spins.argtypes = [p, c_int, p, c_int, p]
+    l.rbim_activate_workspace_bytes.restype = c_size
+    l.rbim_activate_workspace_bytes.argtypes = [c_i64]
+    l.rbim_activate.restype = c_int
+    l.rbim_activate.argtypes = [c_i64, p, p, c_u64, c_u64, c_u64, p, p, c_size, p]
+    l.rbim_label_wrap_workspace_bytes.restype = c_size
+    l.rbim_label_wrap_workspace_bytes.argtypes = [c_i64]
+    l.rbim_label_wrap.restype = c_int
+    l.rbim_label_wrap.argtypes = [c_i64, c_int, p, p, p, p, p, p, c_size, p]
+    l.rbim_batched_workspace_bytes.restype = c_size
+    l.rbim_batched_workspace_bytes.argtypes = []
+    l.rbim_sweeps_batched.restype = c_int
+    l.rbim_sweeps_batched.argtypes = [p, c_int, c_i64, p, p, p, p, p, c_int, c_int, p, p, c_size, p]
+    l.rbim_plain_workspace_bytes.restype = c_size
+    l.rbim_plain_workspace_bytes.argtypes = [c_i64]
+    l.rbim_sweeps_plain.restype = c_int
+    l.rbim_sweeps_plain.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p, c_size, p]
+
+
+def lib(build_if_missing: bool = True):
+    """The loaded library (built from ``csrc/`` first if it is missing or stale)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = _build.LIB
+        if build_if_missing:
+            try:
+                path = _build.build()
+            except Exception as exc:  # pragma: no cover - depends on the toolchain
+                if not os.path.exists(path):
+                    raise RbimError(f"librbim_sm100.so is missing and could not be built: {exc}") from exc
+        if not os.path.exists(path):
+            raise RbimError(f"librbim_sm100.so not found at {path}")
+        l = ctypes.CDLL(path)
+        _declare(l)
+        _lib = l
+        return l
+
+
+def check(rc: int, what: str) -> None:
+    """Raise :class:`RbimError` with the library's message when ``rc`` is not RBIM_OK."""
+    if rc != 0:
+        msg = lib().rbim_last_error().decode(errors="replace")
+        raise RbimError(f"{what} failed ({rc}): {msg}")
+
+
+def plane_words(L: int) -> int:
+    """Words of one bit plane (``rbim_plane_words``)."""
+    return int(lib().rbim_plane_words(int(L)))
+
+
+def resident_max_l() -> int:
+    """Largest L the on-chip engine takes (``rbim_resident_max_l``)."""
+    return int(lib().rbim_resident_max_l())

@@ -1,0 +1,234 @@
+// C ABI of librbim_sm100 (declared in include/rbim_sm100.h): argument checks,
+// error reporting and dispatch to the resident and plain engines.
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "rbim_internal.h"
+#include "rbim_phases.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return RBIM_OK;
+    return fail(RBIM_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+int64_t plane_words(int64_t L) { return (((L * L + 31) / 32) + 3) & ~int64_t(3); }
+
+// Hot-start or cold spins: word w of chain c is word (w & 3) of Philox block
+// w >> 2 of stream 2 (sites 32w .. 32w+31), masked to the lattice.
+__global__ void k_init_spins(const rbim_chain_t *chains, uint32_t *spin_pool, int hot)
+{
+    const rbim_chain_t *c = chains + blockIdx.x;
+    const uint32_t L = (uint32_t)c->L;
+    const rbim::Geom g{L, L * L, (L * L + 31u) / 32u};
+    uint32_t *s = spin_pool + c->spin_off;
+    const uint32_t nwp = (g.NW + 3u) & ~3u;
+    for (uint32_t w = threadIdx.x; w < nwp; w += blockDim.x) {
+        uint32_t v = 0;
+        if (hot && w < g.NW) {
+            const rbim::U4 r = rbim::philox_block(c->key, w >> 2, 0, rbim::kStreamInit);
+            v = rbim::u4_word(r, w & 3u) & g.valid(w);
+        }
+        s[w] = w < g.NW ? v : 0u;
+    }
+}
+
+struct ActWs {
+    uint32_t *OH, *OV, *SEAMV;
+};
+
+ActWs act_ws(void *base, int64_t L)
+{
+    const size_t plane = 4 * (size_t)(plane_words(L) + 4);
+    char *p = (char *)base;
+    return {(uint32_t *)p, (uint32_t *)(p + plane), (uint32_t *)(p + 2 * plane)};
+}
+
+size_t act_ws_bytes(int64_t L) { return 2 * 4 * (size_t)(plane_words(L) + 4) + 4 * (size_t)((L + 31) / 32 + 4); }
+
+__global__ void k_act_clear(ActWs ws, uint32_t L)
+{
+    for (uint32_t i = threadIdx.x; i < (L + 31u) / 32u; i += blockDim.x) ws.SEAMV[i] = 0u;
+}
+
+__global__ void __launch_bounds__(256) k_act_run(ActWs ws, uint32_t L, const uint32_t *S, const uint32_t *J,
+                                                  uint64_t key, uint64_t thr, uint64_t sweep)
+{
+    rbim::Lat<rbim::Word64> t{};
+    t.g = rbim::Geom{L, L * L, (L * L + 31u) / 32u};
+    t.S = const_cast<uint32_t *>(S);
+    t.JH = J;
+    t.JV = J + ((t.g.NW + 3u) & ~3u);
+    t.OH = ws.OH;
+    t.OV = ws.OV;
+    t.SEAMV = ws.SEAMV;
+    t.FLIP = nullptr;  // flip bits are not part of the activation seam
+    rbim::SweepRng rng;
+    rng.key = key;
+    rng.sweep = sweep;
+    rng.thr_any = thr > 0;
+    rng.thr_m1 = thr > 0 ? (uint32_t)min(thr - 1ull, 0xFFFFFFFFull) : 0u;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    rbim::phase_activate_bonds<rbim::Word64>(t, rng, gt >> 5, nt >> 5);
+}
+
+__global__ void k_act_expand(ActWs ws, uint32_t L, uint8_t *occ)
+{
+    const uint32_t N = L * L;
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+        const uint32_t w = n >> 5, b = n & 31u;
+        occ[2ull * n] = (uint8_t)((ws.OH[w] >> b) & 1u);
+        uint32_t v = (ws.OV[w] >> b) & 1u;
+        if (n % L == L - 1u) v = (ws.SEAMV[(n / L) >> 5] >> ((n / L) & 31u)) & 1u;
+        occ[2ull * n + 1] = (uint8_t)v;
+    }
+}
+
+int check_chain_sizes(int64_t L)
+{
+    if (L < 3) return fail(RBIM_ERR_INVALID, "L must be at least 3 (got %lld)", (long long)L);
+    if (L > 32768) return fail(RBIM_ERR_UNSUPPORTED, "L = %lld exceeds the engine's limit of 32768", (long long)L);
+    return RBIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rbim_last_error(void) { return g_last_error.c_str(); }
+
+int rbim_abi_version(void) { return RBIM_ABI_VERSION; }
+
+int64_t rbim_plane_words(int64_t L) { return L < 1 ? 0 : plane_words(L); }
+
+int rbim_resident_max_l(void) { return rbim::resident_max_l(); }
+
+int rbim_init_spins(const rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, int hot, void *stream)
+{
+    if (n_chains < 0) return fail(RBIM_ERR_INVALID, "n_chains must be >= 0");
+    if (n_chains == 0) return RBIM_OK;
+    if (!chains || !spin_pool) return fail(RBIM_ERR_INVALID, "null pointer");
+    if (!aligned16(spin_pool)) return fail(RBIM_ERR_INVALID, "spin_pool must be 16-byte aligned");
+    k_init_spins<<<n_chains, 256, 0, (cudaStream_t)stream>>>(chains, spin_pool, hot);
+    return cuda_check(cudaGetLastError(), "rbim_init_spins");
+}
+
+size_t rbim_activate_workspace_bytes(int64_t L) { return L < 3 ? 0 : act_ws_bytes(L); }
+
+int rbim_activate(int64_t L, const uint32_t *spins, const uint32_t *couplings, uint64_t key, uint64_t thr,
+                  uint64_t sweep, uint8_t *occ, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (int rc = check_chain_sizes(L)) return rc;
+    if (!spins || !couplings || !occ || !workspace) return fail(RBIM_ERR_INVALID, "null pointer");
+    if (thr > (1ull << 32)) return fail(RBIM_ERR_INVALID, "thr must be <= 2^32");
+    if (workspace_bytes < act_ws_bytes(L))
+        return fail(RBIM_ERR_INVALID, "workspace too small: %zu < %zu", workspace_bytes, act_ws_bytes(L));
+    if (!aligned16(workspace)) return fail(RBIM_ERR_INVALID, "workspace must be 16-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    const ActWs ws = act_ws(workspace, L);
+    const uint32_t l = (uint32_t)L;
+    const uint32_t chunks = (l * l + 63u) / 64u;
+    const uint32_t blocks = (chunks + 7u) / 8u;  // one chunk per warp, 8 warps per block
+    k_act_clear<<<1, 256, 0, s>>>(ws, l);
+    k_act_run<<<blocks, 256, 0, s>>>(ws, l, spins, couplings, key, thr, sweep);
+    k_act_expand<<<(l * l + 255u) / 256u, 256, 0, s>>>(ws, l, occ);
+    return cuda_check(cudaGetLastError(), "rbim_activate");
+}
+
+size_t rbim_label_wrap_workspace_bytes(int64_t L)
+{
+    if (L < 3) return 0;
+    if (L <= rbim::resident_max_l()) return 0;
+    return rbim::plain_workspace_bytes(L);
+}
+
+int rbim_label_wrap(int64_t L, int n_lattices, const uint8_t *occ, int32_t *labels, int32_t *n_clusters,
+                    uint8_t *wraps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (int rc = check_chain_sizes(L)) return rc;
+    if (n_lattices < 0) return fail(RBIM_ERR_INVALID, "n_lattices must be >= 0");
+    if (n_lattices == 0) return RBIM_OK;
+    if (!occ || !labels || !n_clusters || !wraps || !status) return fail(RBIM_ERR_INVALID, "null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (L <= rbim::resident_max_l()) {
+        return cuda_check(
+            rbim::launch_resident_label((int)L, n_lattices, occ, labels, n_clusters, wraps, 0, status, s),
+            "rbim_label_wrap (resident)");
+    }
+    const size_t need = rbim::plain_workspace_bytes(L);
+    if (!workspace || workspace_bytes < need)
+        return fail(RBIM_ERR_INVALID, "workspace too small: %zu < %zu", workspace_bytes, need);
+    if (((uintptr_t)workspace & 255u) != 0) return fail(RBIM_ERR_INVALID, "workspace must be 256-byte aligned");
+    const size_t n = (size_t)L * (size_t)L;
+    for (int i = 0; i < n_lattices; ++i) {
+        cudaError_t e = rbim::launch_plain_label(L, occ + 2 * n * i, labels + n * i, n_clusters + i, wraps + 2 * i,
+                                                 status, workspace, s);
+        if (e != cudaSuccess) return cuda_check(e, "rbim_label_wrap (plain)");
+    }
+    return RBIM_OK;
+}
+
+size_t rbim_batched_workspace_bytes(void) { return 256; }
+
+int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
+                        const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
+                        int n_sweeps, int threads, int32_t *status, void *workspace, size_t workspace_bytes,
+                        void *stream)
+{
+    if (n_chains < 0 || n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_chains and n_sweeps must be >= 0");
+    if (n_chains == 0 || n_sweeps == 0) return RBIM_OK;
+    if (int rc = check_chain_sizes(l_max)) return rc;
+    if (l_max > rbim::resident_max_l())
+        return fail(RBIM_ERR_UNSUPPORTED, "l_max = %lld exceeds the resident engine's limit %d", (long long)l_max,
+                    rbim::resident_max_l());
+    if (!chains || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status || !workspace)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    if (!aligned16(spin_pool) || !aligned16(coupling_pool))
+        return fail(RBIM_ERR_INVALID, "spin and coupling pools must be 16-byte aligned");
+    if (workspace_bytes < rbim_batched_workspace_bytes()) return fail(RBIM_ERR_INVALID, "workspace too small");
+    if (threads != 0 && threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+        return fail(RBIM_ERR_INVALID, "threads must be 0, 128, 256, 512 or 1024 (got %d)", threads);
+    cudaError_t e = rbim::launch_resident_sweeps(chains, n_chains, (int)l_max, spin_pool, coupling_pool,
+                                                 (long long *)acc_int, acc_f64, records, n_sweeps, threads, 0,
+                                                 (int *)workspace, status, (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_batched");
+}
+
+size_t rbim_plain_workspace_bytes(int64_t L) { return L < 3 ? 0 : rbim::plain_workspace_bytes(L); }
+
+int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                      int64_t *acc_int, double *acc_f64, int32_t *records, int n_sweeps, int32_t *status,
+                      void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (int rc = check_chain_sizes(L)) return rc;
+    if (n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_sweeps must be >= 0");
+    if (n_sweeps == 0) return RBIM_OK;
+    if (!chain || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status || !workspace)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    const size_t need = rbim::plain_workspace_bytes(L);
+    if (workspace_bytes < need) return fail(RBIM_ERR_INVALID, "workspace too small: %zu < %zu", workspace_bytes, need);
+    if (((uintptr_t)workspace & 255u) != 0) return fail(RBIM_ERR_INVALID, "workspace must be 256-byte aligned");
+    cudaError_t e = rbim::launch_plain_sweeps(chain, spin_pool, coupling_pool, (long long *)acc_int, acc_f64,
+                                              records, n_sweeps, status, workspace, L, (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_plain");
+}
+
+}  // extern "C"

@@ -1,0 +1,466 @@
+// Plain engine: one lattice, any L >= 3, union-find words in global memory
+// (L2-resident up to L ~ 2000), one launch per phase.  It is the drop-in for
+// a single run_single_realization task (src/rbim/simulation.py:148-242) and
+// the path for lattices too large to keep on chip.  Every kernel reads the
+// chain descriptor from device memory, so a whole sequence of sweeps can be
+// enqueued (or captured in a CUDA graph) without host round trips; kernels of
+// a chain that has finished its run return immediately.
+#include <algorithm>
+
+#include "rbim_internal.h"
+#include "rbim_phases.cuh"
+
+namespace rbim {
+
+namespace {
+
+constexpr int kPlainThreads = 256;
+
+struct PlainScratch {
+    int wrap;
+    int err;
+    unsigned int nroots;
+    unsigned int pad0;
+    unsigned long long unsat;
+    unsigned long long downs;
+    long long mc;
+    unsigned long long g1;
+    unsigned long long s1;
+    unsigned long long s2;
+};
+
+struct PlainWs {
+    unsigned long long *uf;
+    uint32_t *OH, *OV, *FLIP, *ROOT, *SEAMV;
+    PlainScratch *sc;
+    unsigned long long *top2;  // 2 per block of the measure kernel
+};
+
+size_t pad256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct PlainSizes {
+    size_t uf, plane, seam, sc, top2, total;
+};
+
+int plain_grid()
+{
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = std::max(1, sms) * 4;
+    }
+    return g;
+}
+
+constexpr int kMaxPlainGrid = 4096;
+
+PlainSizes plain_sizes(int64_t L)
+{
+    PlainSizes s{};
+    const size_t n = (size_t)L * (size_t)L;
+    const size_t nw = ((n + 31) / 32 + 3) & ~size_t(3);
+    s.uf = pad256(8 * n);
+    s.plane = pad256(4 * (nw + 4));
+    s.seam = pad256(4 * ((L + 31) / 32 + 4));
+    s.sc = pad256(sizeof(PlainScratch));
+    s.top2 = pad256(16 * kMaxPlainGrid);
+    s.total = s.uf + 4 * s.plane + s.seam + s.sc + s.top2;
+    return s;
+}
+
+PlainWs plain_ws(void *base, int64_t L)
+{
+    const PlainSizes s = plain_sizes(L);
+    char *p = (char *)base;
+    PlainWs w;
+    w.uf = (unsigned long long *)p;
+    p += s.uf;
+    w.OH = (uint32_t *)p;
+    p += s.plane;
+    w.OV = (uint32_t *)p;
+    p += s.plane;
+    w.FLIP = (uint32_t *)p;
+    p += s.plane;
+    w.ROOT = (uint32_t *)p;
+    p += s.plane;
+    w.SEAMV = (uint32_t *)p;
+    p += s.seam;
+    w.sc = (PlainScratch *)p;
+    p += s.sc;
+    w.top2 = (unsigned long long *)p;
+    return w;
+}
+
+struct PlainArgs {
+    rbim_chain_t *chain;
+    uint32_t *spin_pool;
+    const uint32_t *coupling_pool;
+    long long *acc_i;
+    double *acc_f;
+    int32_t *records;
+    int *status;
+    PlainWs ws;
+};
+
+// Phase of the chain's current sweep: 0 = finished, 1 = thermalisation, 2 = measured.
+__device__ __forceinline__ int chain_phase(const rbim_chain_t *c)
+{
+    const uint64_t s = *((volatile const uint64_t *)&c->sweep);
+    const uint64_t end = (uint64_t)c->n_therm + (uint64_t)c->n_bins * (uint64_t)c->sweeps_per_bin;
+    if (s >= end) return 0;
+    return s >= (uint64_t)c->n_therm ? 2 : 1;
+}
+
+__device__ __forceinline__ Lat<Word64> plain_lat(const PlainArgs &a)
+{
+    Lat<Word64> t;
+    const uint32_t L = (uint32_t)a.chain->L;
+    t.g = Geom{L, L * L, (L * L + 31u) / 32u};
+    t.uf.w = a.ws.uf;
+    t.S = a.spin_pool + a.chain->spin_off;
+    t.JH = a.coupling_pool + a.chain->coupling_off;
+    t.JV = t.JH + ((t.g.NW + 3u) & ~3u);
+    t.OH = a.ws.OH;
+    t.OV = a.ws.OV;
+    t.FLIP = a.ws.FLIP;
+    t.ROOT = a.ws.ROOT;
+    t.SEAMV = a.ws.SEAMV;
+    t.wrap = &a.ws.sc->wrap;
+    t.err = &a.ws.sc->err;
+    t.cap = t.g.N + 64u;
+    return t;
+}
+
+__device__ __forceinline__ uint32_t gwarp() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ uint32_t gnwarps() { return (gridDim.x * blockDim.x) >> 5; }
+__device__ __forceinline__ uint32_t gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t gnthreads() { return gridDim.x * blockDim.x; }
+
+__global__ void k_plain_begin(PlainArgs a)
+{
+    const uint32_t L = (uint32_t)a.chain->L;
+    for (uint32_t i = gtid(); i < (L + 31u) / 32u; i += gnthreads()) a.ws.SEAMV[i] = 0u;
+    if (gtid() == 0) {
+        PlainScratch z{};
+        *a.ws.sc = z;
+    }
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_activate(PlainArgs a)
+{
+    if (!chain_phase(a.chain)) return;
+    const Lat<Word64> t = plain_lat(a);
+    SweepRng rng;
+    rng.key = a.chain->key;
+    rng.sweep = a.chain->sweep;
+    rng.thr_any = a.chain->thr > 0;
+    rng.thr_m1 = a.chain->thr > 0 ? (uint32_t)min(a.chain->thr - 1ull, 0xFFFFFFFFull) : 0u;
+    phase_activate<Word64>(t, rng, gwarp(), gnwarps(), gtid(), gnthreads());
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_heads(PlainArgs a)
+{
+    if (!chain_phase(a.chain)) return;
+    phase_heads<Word64>(plain_lat(a), gwarp(), gnwarps());
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_union(PlainArgs a)
+{
+    if (!chain_phase(a.chain)) return;
+    phase_union<Word64>(plain_lat(a), gwarp(), gnwarps(), gtid(), gnthreads());
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_finalize(PlainArgs a)
+{
+    const int ph = chain_phase(a.chain);
+    if (!ph) return;
+    const Lat<Word64> t = plain_lat(a);
+    const uint32_t nr = phase_finalize<Word64>(t, gwarp(), gnwarps(), true, ph == 2);
+    if ((threadIdx.x & 31u) == 0 && nr) atomicAdd(&a.ws.sc->nroots, nr);
+    for (uint32_t i = gtid(); i < (t.g.L + 31u) / 32u; i += gnthreads()) t.SEAMV[i] = 0u;
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
+{
+    if (chain_phase(a.chain) != 2) return;
+    const Lat<Word64> t = plain_lat(a);
+    uint32_t unsat = 0, downs = 0;
+    measure_energy(t.g, t.S, t.JH, t.JV, gtid(), gnthreads(), unsat, downs);
+    unsigned long long k1 = 0, k2 = 0;
+    for (uint32_t w = gtid(); w < t.g.NW; w += gnthreads()) {
+        uint32_t roots = t.ROOT[w];
+        while (roots) {
+            const uint32_t b = __ffs(roots) - 1u;
+            roots &= roots - 1u;
+            const uint32_t r = (w << 5) + b;
+            const unsigned long long key =
+                ((unsigned long long)Word64::count(t.uf.ld(r)) << 32) | (0xFFFFFFFFull - r);
+            top2_merge(k1, k2, key, 0ull);
+        }
+    }
+    warp_top2(k1, k2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsat += __shfl_xor_sync(0xFFFFFFFFu, unsat, o);
+        downs += __shfl_xor_sync(0xFFFFFFFFu, downs, o);
+    }
+    __shared__ unsigned long long s1[kPlainThreads / 32], s2[kPlainThreads / 32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s1[warp] = k1;
+        s2[warp] = k2;
+        if (unsat) atomicAdd(&a.ws.sc->unsat, (unsigned long long)unsat);
+        if (downs) atomicAdd(&a.ws.sc->downs, (unsigned long long)downs);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long b1 = lane < kPlainThreads / 32 ? s1[lane] : 0ull;
+        unsigned long long b2 = lane < kPlainThreads / 32 ? s2[lane] : 0ull;
+        warp_top2(b1, b2);
+        if (lane == 0) {
+            a.ws.top2[2 * blockIdx.x] = b1;
+            a.ws.top2[2 * blockIdx.x + 1] = b2;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_plain_measure2(PlainArgs a, int nblocks)
+{
+    if (chain_phase(a.chain) != 2) return;
+    unsigned long long k1 = 0, k2 = 0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) top2_merge(k1, k2, a.ws.top2[2 * i], a.ws.top2[2 * i + 1]);
+    warp_top2(k1, k2);
+    __shared__ unsigned long long s1[32], s2[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s1[warp] = k1;
+        s2[warp] = k2;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t nw = blockDim.x >> 5;
+        unsigned long long b1 = lane < nw ? s1[lane] : 0ull, b2 = lane < nw ? s2[lane] : 0ull;
+        warp_top2(b1, b2);
+        if (lane == 0) {
+            PlainScratch *sc = a.ws.sc;
+            sc->g1 = 0xFFFFFFFFull - (b1 & 0xFFFFFFFFull);
+            sc->s1 = b1 >> 32;
+            sc->s2 = b2 >> 32;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_measure3(PlainArgs a)
+{
+    if (chain_phase(a.chain) != 2) return;
+    if (a.ws.sc->nroots <= 1) return;
+    const Lat<Word64> t = plain_lat(a);
+    const uint32_t g1 = (uint32_t)a.ws.sc->g1;
+    const uint32_t lane = threadIdx.x & 31u;
+    int mc = 0;
+    for (uint32_t w = gwarp(); w < t.g.NW; w += gnwarps()) {
+        const uint32_t n = (w << 5) + lane;
+        const bool in = n < t.g.N && Word64::parent(t.uf.ld(n)) == g1;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
+        if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
+    }
+    if (lane == 0 && mc) atomicAdd((unsigned long long *)&a.ws.sc->mc, (unsigned long long)(long long)mc);
+}
+
+__global__ void k_plain_end(PlainArgs a)
+{
+    const int ph = chain_phase(a.chain);
+    if (!ph) return;
+    rbim_chain_t *c = a.chain;
+    PlainScratch *sc = a.ws.sc;
+    if (ph == 2) {
+        const long long N = c->L * c->L;
+        const long long M = N - 2ll * (long long)sc->downs;
+        const long long ncl = sc->nroots;
+        long long s1 = (long long)sc->s1, s2 = (long long)sc->s2, mc = sc->mc;
+        if (ncl == 1) {
+            s1 = N;
+            s2 = 0;
+            mc = M;
+        }
+        if (mc < 0) mc = -mc;
+        const long long E = 2ll * (long long)sc->unsat - 2ll * N;
+        const int wx = sc->wrap & 1, wy = (sc->wrap >> 1) & 1;
+        const long long idx = (long long)(c->sweep - (uint64_t)c->n_therm);
+        const long long bin = idx / c->sweeps_per_bin;
+        Acc acc;
+        acc.zero();
+        acc.add(E, M, ncl, s1, mc, s2, wx, wy);
+        acc.flush(a.acc_i + (c->acc_off + bin) * kAccInt, a.acc_f + (c->acc_off + bin) * kAccF64);
+        if (a.records && c->rec_off >= 0) {
+            int32_t *row = a.records + (c->rec_off + idx) * kRecLen;
+            row[0] = (int32_t)E;
+            row[1] = (int32_t)M;
+            row[2] = (int32_t)ncl;
+            row[3] = (int32_t)s1;
+            row[4] = (int32_t)mc;
+            row[5] = (int32_t)s2;
+            row[6] = wx;
+            row[7] = wy;
+        }
+    }
+    if (sc->err) atomicOr(a.status, sc->err);
+    c->sweep = c->sweep + 1;
+    PlainScratch z{};
+    *sc = z;
+}
+
+// Labelling of a frozen occupation mask (bond-order bytes) through the plain
+// engine's phases, for lattices too large for the resident engine.
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_load(PlainWs ws, uint32_t L, const uint8_t *occ)
+{
+    const Geom g{L, L * L, (L * L + 31u) / 32u};
+    for (uint32_t w = gtid(); w < g.NW; w += gnthreads()) {
+        uint32_t h = 0, v = 0;
+        for (uint32_t b = 0; b < 32u; ++b) {
+            const uint32_t n = (w << 5) + b;
+            if (n >= g.N) break;
+            h |= (occ[2ull * n] ? 1u : 0u) << b;
+            v |= (occ[2ull * n + 1] ? 1u : 0u) << b;
+        }
+        const uint32_t re = g.row_end(w);
+        ws.OH[w] = h;
+        ws.OV[w] = v & ~re;
+        uint32_t seam = v & re;
+        while (seam) {
+            const uint32_t b = __ffs(seam) - 1u;
+            seam &= seam - 1u;
+            const uint32_t x = ((w << 5) + b) / L;
+            atomicOr(ws.SEAMV + (x >> 5), 1u << (x & 31u));
+        }
+    }
+}
+
+__device__ __forceinline__ Lat<Word64> label_lat(const PlainWs &ws, uint32_t L)
+{
+    Lat<Word64> t;
+    t.g = Geom{L, L * L, (L * L + 31u) / 32u};
+    t.uf.w = ws.uf;
+    t.S = nullptr;
+    t.JH = nullptr;
+    t.JV = nullptr;
+    t.OH = ws.OH;
+    t.OV = ws.OV;
+    t.FLIP = ws.FLIP;
+    t.ROOT = ws.ROOT;
+    t.SEAMV = ws.SEAMV;
+    t.wrap = &ws.sc->wrap;
+    t.err = &ws.sc->err;
+    t.cap = t.g.N + 64u;
+    return t;
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_heads(PlainWs ws, uint32_t L)
+{
+    phase_heads<Word64>(label_lat(ws, L), gwarp(), gnwarps());
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_union(PlainWs ws, uint32_t L)
+{
+    phase_union<Word64>(label_lat(ws, L), gwarp(), gnwarps(), gtid(), gnthreads());
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_finalize(PlainWs ws, uint32_t L)
+{
+    phase_finalize<Word64>(label_lat(ws, L), gwarp(), gnwarps(), false, false);
+}
+
+// Exclusive prefix of root counts per word (single CTA) into the FLIP plane.
+__global__ void __launch_bounds__(1024) k_plain_label_scan(PlainWs ws, uint32_t L)
+{
+    __shared__ uint32_t s_scan[1024];
+    const uint32_t NW = (L * L + 31u) / 32u;
+    const uint32_t tid = threadIdx.x, per = (NW + 1023u) / 1024u;
+    const uint32_t w0 = tid * per, w1 = min(NW, w0 + per);
+    uint32_t local = 0;
+    for (uint32_t w = w0; w < w1; ++w) local += __popc(ws.ROOT[w]);
+    s_scan[tid] = local;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024u; off <<= 1) {
+        const uint32_t v = tid >= off ? s_scan[tid - off] : 0u;
+        __syncthreads();
+        s_scan[tid] += v;
+        __syncthreads();
+    }
+    uint32_t base = s_scan[tid] - local;
+    for (uint32_t w = w0; w < w1; ++w) {
+        ws.FLIP[w] = base;
+        base += __popc(ws.ROOT[w]);
+    }
+    if (tid == 0) ws.sc->nroots = s_scan[1023];
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_write(PlainWs ws, uint32_t L, int32_t *labels,
+                                                                     int32_t *n_clusters, uint8_t *wraps,
+                                                                     int *status)
+{
+    const uint32_t N = L * L;
+    for (uint32_t n = gtid(); n < N; n += gnthreads()) {
+        const uint32_t r = Word64::parent(*((volatile unsigned long long *)(ws.uf + n)));
+        labels[n] = (int32_t)(ws.FLIP[r >> 5] + __popc(ws.ROOT[r >> 5] & ((1u << (r & 31u)) - 1u)));
+    }
+    if (gtid() == 0) {
+        *n_clusters = (int32_t)ws.sc->nroots;
+        wraps[0] = (uint8_t)(ws.sc->wrap & 1);
+        wraps[1] = (uint8_t)((ws.sc->wrap >> 1) & 1);
+        if (ws.sc->err) atomicOr(status, ws.sc->err);
+    }
+}
+
+__global__ void k_plain_label_begin(PlainWs ws, uint32_t L)
+{
+    for (uint32_t i = gtid(); i < (L + 31u) / 32u; i += gnthreads()) ws.SEAMV[i] = 0u;
+    if (gtid() == 0) {
+        PlainScratch z{};
+        *ws.sc = z;
+    }
+}
+
+}  // namespace
+
+size_t plain_workspace_bytes(int64_t L) { return plain_sizes(L).total; }
+
+cudaError_t launch_plain_sweeps(rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                                long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *status,
+                                void *workspace, int64_t L, cudaStream_t stream)
+{
+    PlainArgs a{chain, spin_pool, coupling_pool, acc_i, acc_f, records, status, plain_ws(workspace, L)};
+    const int grid = std::min(plain_grid(), kMaxPlainGrid);
+    k_plain_begin<<<1, 256, 0, stream>>>(a);
+    for (int s = 0; s < n_sweeps; ++s) {
+        k_plain_activate<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_heads<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_union<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_finalize<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_measure1<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_measure2<<<1, 1024, 0, stream>>>(a, grid);
+        k_plain_measure3<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_end<<<1, 1, 0, stream>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_label(int64_t L, const uint8_t *occ, int32_t *labels, int32_t *n_clusters,
+                               uint8_t *wraps, int *status, void *workspace, cudaStream_t stream)
+{
+    const PlainWs ws = plain_ws(workspace, L);
+    const int grid = std::min(plain_grid(), kMaxPlainGrid);
+    const uint32_t l = (uint32_t)L;
+    k_plain_label_begin<<<1, 256, 0, stream>>>(ws, l);
+    k_plain_label_load<<<grid, kPlainThreads, 0, stream>>>(ws, l, occ);
+    k_plain_label_heads<<<grid, kPlainThreads, 0, stream>>>(ws, l);
+    k_plain_label_union<<<grid, kPlainThreads, 0, stream>>>(ws, l);
+    k_plain_label_finalize<<<grid, kPlainThreads, 0, stream>>>(ws, l);
+    k_plain_label_scan<<<1, 1024, 0, stream>>>(ws, l);
+    k_plain_label_write<<<grid, kPlainThreads, 0, stream>>>(ws, l, labels, n_clusters, wraps, status);
+    return cudaGetLastError();
+}
+
+}  // namespace rbim

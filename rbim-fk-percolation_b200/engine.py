@@ -1,0 +1,276 @@
+"""Device-resident chain sets and the two sweep engines behind the C ABI.
+
+A *chain* is one disorder realization at one temperature, the task unit of the
+reference's ``run_temperature_scan`` (``simulation.py:384-399``).  A
+:class:`ChainSet` owns, in device memory, the spin planes of its chains, the
+coupling planes of their realizations (shared by every temperature of a
+realization), the ``rbim_chain_t`` descriptors, the per-bin accumulators and
+optional per-sweep records; only accumulators (and, on request, spins and
+records) ever come back to the host.  PyTorch provides the device memory and
+the stream; every computation is a call into ``librbim_sm100.so``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from .packing import threshold, unpack_spins, words_for
+
+__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda"]
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def require_cuda(device=None):
+    """Return the CUDA device to use; raise if there is none (no CPU fallback exists)."""
+    torch = _torch()
+    if not torch.cuda.is_available():
+        raise _native.RbimError("the rbim B200 engine needs a CUDA device; none is available")
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise _native.RbimError(f"the rbim B200 engine runs on CUDA devices only, got {d}")
+    return d
+
+
+def chain_key(seed) -> int:
+    """64-bit Philox key of a chain from an int, a ``SeedSequence`` or ``None``.
+
+    The reference seeds each task with a ``SeedSequence`` child
+    (``simulation.py:367-368, 384-393``); the engine turns that child into its
+    key with ``generate_state(2, uint32)``.
+    """
+    ss = seed if isinstance(seed, np.random.SeedSequence) else np.random.SeedSequence(seed)
+    w = ss.generate_state(2, dtype=np.uint32)
+    return int(w[0]) | (int(w[1]) << 32)
+
+
+@dataclass
+class ChainSpec:
+    """One chain: lattice size, index of its realization, key, inverse temperature, run layout."""
+
+    L: int
+    realization: int
+    key: int
+    beta: float
+    n_therm: int
+    n_bins: int
+    sweeps_per_bin: int
+    records: bool = False
+
+    @property
+    def n_total(self) -> int:
+        return self.n_therm + self.n_bins * self.sweeps_per_bin
+
+
+class ChainSet:
+    """Device state of many chains plus the calls that advance them.
+
+    ``couplings`` holds one packed coupling array (``pack_couplings``) per
+    realization; ``specs[i].realization`` indexes it.
+    """
+
+    def __init__(self, specs: Sequence[ChainSpec], couplings: Sequence[np.ndarray], device=None):
+        torch = _torch()
+        self.device = require_cuda(device)
+        self.lib = _native.lib()
+        self.specs = list(specs)
+        if not self.specs:
+            raise ValueError("a ChainSet needs at least one chain")
+        self.n = len(self.specs)
+        Ls = np.array([s.L for s in self.specs], dtype=np.int64)
+        if np.any(Ls < 3):
+            raise ValueError("L must be at least 3")
+        self.l_max = int(Ls.max())
+        real_L = {}
+        for s in self.specs:
+            if s.realization < 0 or s.realization >= len(couplings):
+                raise ValueError(f"chain refers to realization {s.realization} of {len(couplings)}")
+            if real_L.setdefault(s.realization, s.L) != s.L:
+                raise ValueError("all chains of one realization must share L")
+            if s.sweeps_per_bin < 1 or s.n_bins < 1 or s.n_therm < 0:
+                raise ValueError("n_bins and sweeps_per_bin must be >= 1 and n_therm >= 0")
+
+        # Coupling pool: realizations back to back (JH plane then JV plane).
+        c_off = np.zeros(len(couplings), dtype=np.int64)
+        total = 0
+        for r, c in enumerate(couplings):
+            L = real_L.get(r)
+            if L is None:
+                c_off[r] = total
+                continue
+            if c.size != 2 * words_for(L):
+                raise ValueError(f"realization {r}: packed couplings have {c.size} words, expected {2 * words_for(L)}")
+            c_off[r] = total
+            total += c.size
+        pool = np.zeros(max(total, 4), dtype="<u4")
+        for r, c in enumerate(couplings):
+            if r in real_L:
+                pool[c_off[r]: c_off[r] + c.size] = c
+        self.coupling_pool = torch.from_numpy(pool.view(np.int32)).to(self.device)
+
+        # Spin pool, accumulators, records.
+        s_off = np.zeros(self.n, dtype=np.int64)
+        a_off = np.zeros(self.n, dtype=np.int64)
+        r_off = np.full(self.n, -1, dtype=np.int64)
+        ts = ta = tr = 0
+        for i, s in enumerate(self.specs):
+            s_off[i] = ts
+            ts += words_for(s.L)
+            a_off[i] = ta
+            ta += s.n_bins
+            if s.records:
+                r_off[i] = tr
+                tr += s.n_bins * s.sweeps_per_bin
+        self.spin_pool = torch.zeros(max(ts, 4), dtype=torch.int32, device=self.device)
+        self.acc_int = torch.zeros((max(ta, 1), _native.ACC_INT), dtype=torch.int64, device=self.device)
+        self.acc_f64 = torch.zeros((max(ta, 1), _native.ACC_F64), dtype=torch.float64, device=self.device)
+        self.records = torch.zeros((tr, _native.REC_LEN), dtype=torch.int32, device=self.device) if tr else None
+        self.spin_off, self.acc_off, self.rec_off = s_off, a_off, r_off
+
+        desc = np.zeros(self.n, dtype=_native.CHAIN_DTYPE)
+        desc["key"] = [s.key for s in self.specs]
+        desc["thr"] = [threshold(s.beta) for s in self.specs]
+        desc["spin_off"] = s_off
+        desc["coupling_off"] = c_off[[s.realization for s in self.specs]]
+        desc["acc_off"] = a_off
+        desc["rec_off"] = r_off
+        desc["n_therm"] = [s.n_therm for s in self.specs]
+        desc["n_bins"] = [s.n_bins for s in self.specs]
+        desc["sweeps_per_bin"] = [s.sweeps_per_bin for s in self.specs]
+        desc["L"] = Ls
+        self.desc_host = desc
+        self.chains = torch.from_numpy(desc.view(np.uint8).copy()).to(self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.n_total = np.array([s.n_total for s in self.specs], dtype=np.int64)
+        self._sweep_host = np.zeros(self.n, dtype=np.int64)
+        self._ws = None
+
+    # -- helpers -----------------------------------------------------------
+    @staticmethod
+    def _ptr(t) -> ctypes.c_void_p:
+        return ctypes.c_void_p(t.data_ptr())
+
+    def _stream(self):
+        return ctypes.c_void_p(_torch().cuda.current_stream(self.device).cuda_stream)
+
+    def _workspace(self, nbytes: int):
+        torch = _torch()
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    # -- state -------------------------------------------------------------
+    def init_spins(self, hot: bool = True) -> None:
+        """Hot (Philox) or cold start of every chain (reference ``initial_spins``)."""
+        with _torch().cuda.device(self.device):
+            rc = self.lib.rbim_init_spins(self._ptr(self.chains), self.n, self._ptr(self.spin_pool), int(hot),
+                                          self._stream())
+        _native.check(rc, "rbim_init_spins")
+
+    def set_spins(self, i: int, words: np.ndarray) -> None:
+        nw = words_for(self.specs[i].L)
+        src = _torch().from_numpy(np.ascontiguousarray(words, dtype="<u4").view(np.int32))
+        self.spin_pool[self.spin_off[i]: self.spin_off[i] + nw].copy_(src)
+
+    def set_sweep(self, i: int, sweep: int) -> None:
+        """Set chain ``i``'s sweep counter (host and device copies)."""
+        self.desc_host["sweep"][i] = sweep
+        row = _torch().from_numpy(self.desc_host[i: i + 1].view(np.uint8).copy())
+        self.chains[96 * i: 96 * (i + 1)].copy_(row)
+        self._sweep_host[i] = min(sweep, self.n_total[i])
+
+    def spin_words(self, i: int) -> np.ndarray:
+        nw = words_for(self.specs[i].L)
+        return self.spin_pool[self.spin_off[i]: self.spin_off[i] + nw].cpu().numpy().view("<u4")
+
+    def spins(self, i: int) -> np.ndarray:
+        return unpack_spins(self.spin_words(i), self.specs[i].L)
+
+    # -- sweeps ------------------------------------------------------------
+    def run_batched(self, n_sweeps: int, threads: int = 0) -> None:
+        """Advance every chain by up to ``n_sweeps`` sweeps on the resident engine (one launch)."""
+        if n_sweeps <= 0:
+            return
+        nbytes = int(self.lib.rbim_batched_workspace_bytes())
+        ws = self._workspace(nbytes)
+        with _torch().cuda.device(self.device):
+            rc = self.lib.rbim_sweeps_batched(
+                self._ptr(self.chains), self.n, self.l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
+                self._ptr(self.acc_int), self._ptr(self.acc_f64),
+                self._ptr(self.records) if self.records is not None else None,
+                int(n_sweeps), int(threads), self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
+        _native.check(rc, "rbim_sweeps_batched")
+        self._sweep_host = np.minimum(self._sweep_host + n_sweeps, self.n_total)
+
+    def run_plain(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> None:
+        """Advance chains one at a time on the plain (global-memory) engine."""
+        if n_sweeps <= 0:
+            return
+        idx = range(self.n) if chains is None else chains
+        nbytes = max(int(self.lib.rbim_plain_workspace_bytes(self.specs[i].L)) for i in idx)
+        ws = self._workspace(nbytes)
+        with _torch().cuda.device(self.device):
+            for i in idx:
+                rc = self.lib.rbim_sweeps_plain(
+                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * i), self._ptr(self.spin_pool),
+                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
+                    self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
+                    self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
+                _native.check(rc, "rbim_sweeps_plain")
+                self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
+
+    def remaining(self) -> int:
+        """Sweeps still to run for the longest chain (host bookkeeping)."""
+        return int(np.max(self.n_total - self._sweep_host))
+
+    def run_to_end(self, engine: str = "auto", chunk: int = 1000, threads: int = 0) -> None:
+        """Run every chain to the end of its run in chunks of ``chunk`` sweeps."""
+        if engine == "auto":
+            engine = "batched" if self.l_max <= _native.resident_max_l() else "plain"
+        if engine not in ("batched", "plain"):
+            raise ValueError(f"engine must be 'auto', 'batched' or 'plain', got {engine!r}")
+        while self.remaining() > 0:
+            n = min(chunk, self.remaining())
+            if engine == "batched":
+                self.run_batched(n, threads)
+            else:
+                self.run_plain(n)
+        self.check_status()
+
+    def check_status(self) -> None:
+        st = int(self.status.item())
+        if st:
+            raise _native.RbimError(f"device status word {st:#x} (1 = find bound, 2 = union bound, 4 = bad chain)")
+
+    # -- results -----------------------------------------------------------
+    def device_sweeps(self) -> np.ndarray:
+        """The chains' sweep counters as stored on the device."""
+        d = self.chains.cpu().numpy().view(_native.CHAIN_DTYPE)
+        return d["sweep"].astype(np.int64)
+
+    def bins(self, i: int):
+        """``(int_sums (n_bins, 12), f64_sums (n_bins, 2))`` of chain ``i`` (host copies)."""
+        s = self.specs[i]
+        a = self.acc_off[i]
+        return (self.acc_int[a: a + s.n_bins].cpu().numpy(), self.acc_f64[a: a + s.n_bins].cpu().numpy())
+
+    def all_bins(self):
+        return self.acc_int.cpu().numpy(), self.acc_f64.cpu().numpy()
+
+    def chain_records(self, i: int) -> np.ndarray:
+        s = self.specs[i]
+        if self.records is None or self.rec_off[i] < 0:
+            raise ValueError(f"chain {i} was created without records")
+        r = self.rec_off[i]
+        return self.records[r: r + s.n_bins * s.sweeps_per_bin].cpu().numpy()

@@ -1,0 +1,83 @@
+"""Conversion between the reference's arrays and the engine's linear bit planes.
+
+A plane stores bit ``n`` (site ``n = x * L + y``) in word ``n >> 5`` at position
+``n & 31``; ``plane_words(L)`` words per lattice (``ceil(L*L/32)`` rounded up to
+a multiple of 4), bits past ``L*L`` zero.  Spins: bit set <=> ``s = -1``.
+Couplings: a JH plane (bond ``2n``) followed by a JV plane (bond ``2n + 1``),
+bit set <=> ``J = -1``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["words_for", "pack_plane", "unpack_plane", "pack_spins", "unpack_spins", "pack_couplings",
+           "unpack_couplings", "threshold"]
+
+
+def words_for(L: int) -> int:
+    """Words of one plane; identical to ``rbim_plane_words`` of the C ABI."""
+    n = L * L
+    return (((n + 31) // 32) + 3) & ~3
+
+
+def pack_plane(bits: np.ndarray, L: int) -> np.ndarray:
+    """Pack a boolean array of ``L*L`` sites into ``words_for(L)`` uint32 words."""
+    b = np.ascontiguousarray(bits, dtype=bool).reshape(-1)
+    if b.size != L * L:
+        raise ValueError(f"expected {L * L} sites, got {b.size}")
+    nw = words_for(L)
+    by = np.zeros(4 * nw, dtype=np.uint8)
+    packed = np.packbits(b, bitorder="little")
+    by[: packed.size] = packed
+    return by.view("<u4").copy()
+
+
+def unpack_plane(words: np.ndarray, L: int) -> np.ndarray:
+    """Inverse of :func:`pack_plane`."""
+    w = np.ascontiguousarray(words, dtype="<u4")
+    return np.unpackbits(w.view(np.uint8), bitorder="little")[: L * L].astype(bool)
+
+
+def pack_spins(spins: np.ndarray, L: int) -> np.ndarray:
+    """``+-1`` spins of shape ``(L*L,)`` -> spin plane."""
+    s = np.asarray(spins).reshape(-1)
+    if not np.all((s == 1) | (s == -1)):
+        raise ValueError("spins must be +-1")
+    return pack_plane(s == -1, L)
+
+
+def unpack_spins(words: np.ndarray, L: int, dtype=np.int64) -> np.ndarray:
+    """Spin plane -> ``+-1`` spins of shape ``(L*L,)``."""
+    return np.where(unpack_plane(words, L), -1, 1).astype(dtype)
+
+
+def pack_couplings(J: np.ndarray, L: int) -> np.ndarray:
+    """Bond-ordered couplings ``(2*L*L,)`` (reference ``couplings_from_disorder``) -> JH plane + JV plane."""
+    j = np.asarray(J).reshape(-1)
+    if j.size != 2 * L * L:
+        raise ValueError(f"expected {2 * L * L} couplings, got {j.size}")
+    if not np.all((j == 1) | (j == -1)):
+        raise ValueError("couplings must be +-1")
+    return np.concatenate([pack_plane(j[0::2] == -1, L), pack_plane(j[1::2] == -1, L)])
+
+
+def unpack_couplings(words: np.ndarray, L: int) -> np.ndarray:
+    nw = words_for(L)
+    J = np.empty(2 * L * L, dtype=np.int8)
+    J[0::2] = np.where(unpack_plane(words[:nw], L), -1, 1)
+    J[1::2] = np.where(unpack_plane(words[nw:2 * nw], L), -1, 1)
+    return J
+
+
+def threshold(beta: float) -> int:
+    """Activation threshold ``floor(p_add * 2^32)`` with ``p_add = -expm1(-2 beta)``.
+
+    ``p_add`` is the reference's ``bond_activation_probability``
+    (``clusters.py:40-45``); a bond is occupied when its Philox word is below the
+    threshold, so ``P(occupied) = thr / 2^32`` is within ``2^-32`` of ``p_add``.
+    """
+    p_add = float(-np.expm1(-2.0 * float(beta)))
+    if not 0.0 <= p_add <= 1.0:
+        raise ValueError(f"activation probability {p_add} outside [0, 1] (beta = {beta})")
+    return int(np.floor(p_add * 4294967296.0))

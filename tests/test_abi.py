@@ -1,0 +1,86 @@
+"""The C ABI library loads and exports every symbol of ``include/rbim_sm100.h`` (no GPU needed).
+
+Only calls that do no device work are made here: size queries, the resident
+limit, and argument checks that must fail before touching CUDA.
+"""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "rbim_sm100.h")
+
+
+def _declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rbim_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree(rb):
+    assert _declared_functions() == sorted(rb._native.EXPORTED_SYMBOLS)
+
+
+def test_library_exports_every_declared_symbol(rb):
+    lib = rb._native.lib()
+    for name in _declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_chain_struct_layout_matches_header(rb):
+    text = open(HEADER).read()
+    body = re.search(r"typedef struct rbim_chain_t \{(.*?)\} rbim_chain_t;", text, re.S).group(1)
+    fields = re.findall(r"(u?int64_t)\s+([A-Za-z_]+);", body)
+    assert [f for _, f in fields] == list(rb._native.CHAIN_DTYPE.names)
+    for (ctype, name) in fields:
+        kind = rb._native.CHAIN_DTYPE[name]
+        assert kind.itemsize == 8 and (kind.kind == "u") == ctype.startswith("u"), name
+
+
+def test_host_only_queries(rb):
+    lib = rb._native.lib()
+    assert lib.rbim_abi_version() == 1
+    assert lib.rbim_plane_words(3) == 4 and lib.rbim_plane_words(64) == 128
+    lmax = lib.rbim_resident_max_l()
+    assert 128 <= lmax <= 256
+    assert lib.rbim_label_wrap_workspace_bytes(lmax) == 0
+    assert lib.rbim_label_wrap_workspace_bytes(lmax + 1) == lib.rbim_plain_workspace_bytes(lmax + 1) > 0
+    assert lib.rbim_plain_workspace_bytes(1024) >= 8 * 1024 * 1024
+    assert lib.rbim_activate_workspace_bytes(2) == 0
+    assert lib.rbim_batched_workspace_bytes() >= 4
+
+
+def test_argument_errors_are_reported_without_device_work(rb):
+    lib = rb._native.lib()
+    p = ctypes.c_void_p
+    rc = lib.rbim_sweeps_batched(None, 4, 32, None, None, None, None, None, 10, 0, None, None, 0, None)
+    assert rc == -1 and b"null pointer" in lib.rbim_last_error()
+    dummy = p(16)
+    rc = lib.rbim_sweeps_batched(dummy, 4, 100000, dummy, dummy, dummy, dummy, None, 10, 0, dummy, dummy, 256, None)
+    assert rc == -3
+    rc = lib.rbim_sweeps_batched(dummy, 4, 32, dummy, dummy, dummy, dummy, None, 10, 384, dummy, dummy, 256, None)
+    assert rc == -1 and b"threads" in lib.rbim_last_error()
+    rc = lib.rbim_sweeps_batched(dummy, 4, 2, dummy, dummy, dummy, dummy, None, 10, 0, dummy, dummy, 256, None)
+    assert rc == -1 and b"at least 3" in lib.rbim_last_error()
+    rc = lib.rbim_sweeps_plain(64, dummy, dummy, dummy, dummy, dummy, None, 5, dummy, dummy, 10, None)
+    assert rc == -1 and b"workspace too small" in lib.rbim_last_error()
+    rc = lib.rbim_label_wrap(8, -1, dummy, dummy, dummy, dummy, dummy, None, 0, None)
+    assert rc == -1
+    rc = lib.rbim_activate(8, dummy, dummy, 1, 2**32 + 1, 0, dummy, dummy, 1 << 20, None)
+    assert rc == -1 and b"thr" in lib.rbim_last_error()
+    # Zero-work calls succeed without touching the device.
+    assert lib.rbim_sweeps_batched(None, 0, 32, None, None, None, None, None, 10, 0, None, None, 0, None) == 0
+    assert lib.rbim_label_wrap(8, 0, None, None, None, None, None, None, 0, None) == 0
+
+
+def test_packing_matches_the_documented_layout(rb):
+    # Site n is bit n & 31 of word n >> 5; a set spin bit means s = -1.
+    L = 6
+    spins = np.ones(L * L, dtype=np.int64)
+    spins[[0, 5, 31, 32, 35]] = -1
+    w = rb.packing.pack_spins(spins, L)
+    assert w[0] == (1 << 0) | (1 << 5) | (1 << 31) and w[1] == (1 << 0) | (1 << 3)

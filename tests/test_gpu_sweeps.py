@@ -1,0 +1,144 @@
+"""Bit-exact parity of activation, sweeps and whole chains against the oracle's Philox replay.
+
+The engine and the oracle draw the same Philox4x32-10 stream, so for a fixed
+key every occupation mask, flip, per-sweep record, per-bin sum and final spin
+configuration must agree exactly; the integer sums are compared as integers
+and the two double sums (M^4, |M_C1|/S1) bit for bit, since both sides add
+the same values in the same order.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _thr(T):
+    return int(np.floor(-np.expm1(-2.0 * (1.0 / T)) * 2**32))
+
+
+def _couplings(L, p, seed):
+    rng = np.random.default_rng(seed)
+    return np.where(rng.random(2 * L * L) < p, -1, 1).astype(np.int8)
+
+
+@pytest.mark.parametrize("L", [3, 5, 16, 33, 64, 100, 250])
+def test_activation_matches_philox_replay(rb, orc, L):
+    rng = np.random.default_rng(L)
+    J = _couplings(L, 0.2, L)
+    spins = np.where(rng.random(L * L) < 0.5, -1, 1).astype(np.int8)
+    lattice = rb.build_lattice(L)
+    for T, sweep in ((0.5, 0), (2.27, 7), (4.0, 2**33 + 5)):
+        got = rb.activate_bonds(spins, lattice, J, 1.0 / T, key=0xABCDEF123 + L, sweep=sweep)
+        want = orc.activate(L, spins, J, key=0xABCDEF123 + L, thr=rb.packing.threshold(1.0 / T), sweep=sweep)
+        assert np.array_equal(got, want), (L, T)
+
+
+def test_activation_limits(rb):
+    """Reference ``tests/test_clusters.py:30-59``: beta = 0 activates nothing, beta = 50 everything satisfied."""
+    L = 8
+    lattice = rb.build_lattice(L)
+    J = np.ones(2 * L * L, dtype=np.int8)
+    spins = np.ones(L * L, dtype=np.int64)
+    assert not rb.activate_bonds(spins, lattice, J, 0.0, key=1).any()
+    full = rb.activate_bonds(spins, lattice, J, 50.0, key=1)
+    assert full.all()
+    n, _, wx, wy = rb.label_and_wrap(full, lattice)
+    assert n == 1 and wx and wy
+
+
+def _chain(rb, orc, Ls, engine, n_therm=5, n_bins=3, spb=7, p=0.1, temps=(1.0, 2.27, 4.0), records=False,
+           chunks=None):
+    specs, couplings, J_host = [], [], []
+    for i, L in enumerate(Ls):
+        J = _couplings(L, p, 100 + i)
+        couplings.append(rb.packing.pack_couplings(J, L))
+        J_host.append(J)
+        T = temps[i % len(temps)]
+        specs.append(rb.ChainSpec(L=L, realization=i, key=(0x1234567 * (i + 1)) & (2**64 - 1), beta=1.0 / T,
+                                  n_therm=n_therm, n_bins=n_bins, sweeps_per_bin=spb, records=records))
+    cs = rb.ChainSet(specs, couplings)
+    cs.init_spins(hot=True)
+    total = n_therm + n_bins * spb
+    for n in chunks or [total]:
+        if engine == "batched":
+            cs.run_batched(n)
+        else:
+            cs.run_plain(n)
+    cs.check_status()
+    assert np.all(cs.device_sweeps() == total)
+    for i, s in enumerate(specs):
+        ib, fb, spins = orc.run_chain(s.L, J_host[i], s.key, rb.packing.threshold(s.beta), hot=True, n_therm=n_therm,
+                                      n_bins=n_bins, sweeps_per_bin=spb)
+        gi, gf = cs.bins(i)
+        assert np.array_equal(gi, ib), (engine, s.L, i)
+        assert np.array_equal(gf.view(np.uint64), fb.view(np.uint64)), (engine, s.L, i)
+        assert np.array_equal(cs.spins(i), spins.astype(np.int64)), (engine, s.L, i)
+    return cs, specs, J_host
+
+
+@pytest.mark.parametrize("L", [3, 4, 8, 16, 32, 48, 64])
+def test_batched_chain_bit_exact(rb, orc, L):
+    _chain(rb, orc, [L] * 6, "batched")
+
+
+@pytest.mark.parametrize("L", [3, 8, 32, 64, 128])
+def test_plain_chain_bit_exact(rb, orc, L):
+    _chain(rb, orc, [L] * 2, "plain")
+
+
+def test_batched_uneven_sizes_one_launch(rb, orc):
+    _chain(rb, orc, [32, 48, 64, 96, 128, 5, 17, 200], "batched", n_therm=3, n_bins=2, spb=4)
+
+
+def test_chunked_calls_equal_one_call(rb, orc):
+    _chain(rb, orc, [24] * 4, "batched", n_therm=4, n_bins=3, spb=5, chunks=[1, 3, 2, 5, 4, 100])
+    _chain(rb, orc, [24] * 2, "plain", n_therm=4, n_bins=3, spb=5, chunks=[2, 7, 100])
+
+
+def test_records_match_oracle_sweeps(rb, orc):
+    L, n_therm, spb = 20, 3, 6
+    for engine in ("batched", "plain"):
+        cs, specs, J_host = _chain(rb, orc, [L] * 3, engine, n_therm=n_therm, n_bins=2, spb=spb, records=True)
+        for i, s in enumerate(specs):
+            recs = cs.chain_records(i)
+            spins = orc.initial_spins(L * L, s.key, hot=True)
+            for t in range(n_therm + 2 * spb):
+                r = orc.sw_sweep(L, spins, J_host[i], s.key, rb.packing.threshold(s.beta), t, measure=t >= n_therm)
+                if t >= n_therm:
+                    want = (r[0], r[1], r[2], r[3], r[4], r[5], r[7], r[8])
+                    assert tuple(int(v) for v in recs[t - n_therm]) == want, (engine, i, t)
+
+
+def test_largest_lattice_on_chip_and_beyond(rb, orc):
+    lmax = rb._native.resident_max_l()
+    _chain(rb, orc, [lmax], "batched", n_therm=1, n_bins=1, spb=2, temps=(1.5,))
+    _chain(rb, orc, [lmax + 1], "plain", n_therm=1, n_bins=1, spb=2, temps=(1.5,))
+
+
+def test_cold_start_and_zero_temperature_limit(rb):
+    """A cold ferromagnet at T -> 0 is one wrapping cluster every sweep."""
+    L = 16
+    J = np.ones(2 * L * L, dtype=np.int8)
+    spec = rb.ChainSpec(L=L, realization=0, key=5, beta=50.0, n_therm=0, n_bins=1, sweeps_per_bin=10, records=True)
+    cs = rb.ChainSet([spec], [rb.packing.pack_couplings(J, L)])
+    cs.init_spins(hot=False)
+    cs.run_batched(10)
+    rec = cs.chain_records(0)
+    assert np.all(rec[:, 2] == 1) and np.all(rec[:, 3] == L * L) and np.all(rec[:, 6] == 1) and np.all(rec[:, 7] == 1)
+    assert np.all(np.abs(rec[:, 1]) == L * L) and np.all(rec[:, 0] == -2 * L * L)
+
+
+def test_sw_sweep_api_matches_oracle(rb, orc):
+    L = 12
+    lattice = rb.build_lattice(L)
+    J = _couplings(L, 0.15, 9)
+    spins = orc.initial_spins(L * L, 77, hot=True).astype(np.int64)
+    ref = spins.astype(np.int8).copy()
+    for t in range(4):
+        res = rb.sw_sweep(spins, lattice, J, 1 / 1.8, key=77, sweep=t)
+        r = orc.sw_sweep(L, ref, J, 77, rb.packing.threshold(1 / 1.8), t, measure=True)
+        assert (res.energy, res.magnetization, res.n_clusters, res.largest_size, res.largest_abs_magnetization,
+                res.second_size, res.wraps_x, res.wraps_y) == (r[0], r[1], r[2], r[3], r[4], r[5], bool(r[7]),
+                                                               bool(r[8]))
+        assert np.array_equal(spins, ref.astype(np.int64))
