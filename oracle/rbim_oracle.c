@@ -25,9 +25,13 @@
  * 3", SC'11), so a whole chain can be replayed bit for bit:
  *
  *   key     = 64-bit chain key, low word key[0], high word key[1]
- *   bond k of sweep t   : word (k & 3) of Philox(ctr = {k >> 2, t_lo, t_hi, 0})
- *                         occupied iff satisfied and word < thr, where
- *                         thr = floor(p_add * 2^32), p_add = -expm1(-2 beta)
+ *   bond k of sweep t   : 32-bit uniform (u << 16) | v, where u is 16-bit
+ *                         halfword (k & 7) of Philox(ctr = {k >> 3, t_lo, t_hi, 0})
+ *                         and v the same halfword of Philox(ctr = {k >> 3, t_lo,
+ *                         t_hi, 3}); halfword h is bits 16*(h&1).. of word h>>1.
+ *                         Occupied iff satisfied and uniform < thr, where
+ *                         thr = floor(p_add * 2^32), p_add = -expm1(-2 beta).
+ *                         (The engine draws v only when u == thr >> 16.)
  *   flip of the cluster whose smallest site is r, sweep t :
  *                         bit (r & 127) of Philox(ctr = {r >> 7, t_lo, t_hi, 1})
  *   hot-start spin of site n : bit (n & 127) of Philox(ctr = {n >> 7, 0, 0, 2});
@@ -92,9 +96,13 @@ static void philox_stream(uint64_t key, uint64_t block, uint64_t sweep, uint32_t
 
 uint32_t orc_bond_uniform(uint64_t key, uint64_t sweep, uint64_t bond)
 {
-    uint32_t out[4];
-    philox_stream(key, bond >> 2, sweep, 0u, out);
-    return out[bond & 3];
+    uint32_t hi[4], lo[4];
+    philox_stream(key, bond >> 3, sweep, 0u, hi);
+    philox_stream(key, bond >> 3, sweep, 3u, lo);
+    const unsigned h = (unsigned)(bond & 7);
+    const uint32_t u = (hi[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
+    const uint32_t v = (lo[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
+    return (u << 16) | v;
 }
 
 int orc_flip_bit(uint64_t key, uint64_t sweep, uint64_t root)
@@ -130,15 +138,39 @@ static inline int64_t bond_end_b(int64_t L, int64_t k)
 /* Bond activation (clusters.py:48-79)                                       */
 /* ------------------------------------------------------------------------ */
 
+/* Bonds are taken eight at a time (one Philox block); the low halves come
+ * from the second stream only when some satisfied bond's high half equals
+ * thr >> 16, which yields the same decisions as comparing every bond's full
+ * orc_bond_uniform with thr. */
 void orc_activate(int64_t L, const int8_t *spins, const int8_t *J, uint64_t key, uint64_t thr,
                   uint64_t sweep, uint8_t *occ)
 {
     int64_t nb = 2 * L * L;
-    for (int64_t k = 0; k < nb; ++k) {
-        int64_t a = k >> 1, b = bond_end_b(L, k);
-        int satisfied = (int)J[k] * (int)spins[a] * (int)spins[b] > 0;
-        uint64_t r = orc_bond_uniform(key, sweep, (uint64_t)k);
-        occ[k] = (uint8_t)(satisfied && r < thr);
+    const uint32_t thr_hi = (uint32_t)(thr >> 16);
+    for (int64_t k0 = 0; k0 < nb; k0 += 8) {
+        uint32_t hi[4], lo[4];
+        int have_lo = 0;
+        philox_stream(key, (uint64_t)k0 >> 3, sweep, 0u, hi);
+        for (int64_t k = k0; k < k0 + 8 && k < nb; ++k) {
+            int64_t a = k >> 1, b = bond_end_b(L, k);
+            int satisfied = (int)J[k] * (int)spins[a] * (int)spins[b] > 0;
+            const unsigned h = (unsigned)(k & 7);
+            const uint32_t u = (hi[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
+            int on = 0;
+            if (satisfied) {
+                if (thr >= (1ull << 32) || u < thr_hi) {
+                    on = 1;
+                } else if (u == thr_hi) {
+                    if (!have_lo) {
+                        philox_stream(key, (uint64_t)k0 >> 3, sweep, 3u, lo);
+                        have_lo = 1;
+                    }
+                    const uint32_t v = (lo[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
+                    on = ((u << 16) | v) < thr;
+                }
+            }
+            occ[k] = (uint8_t)on;
+        }
     }
 }
 

@@ -81,11 +81,7 @@ __global__ void __launch_bounds__(256) k_act_run(ActWs ws, uint32_t L, const uin
     t.OV = ws.OV;
     t.SEAMV = ws.SEAMV;
     t.FLIP = nullptr;  // flip bits are not part of the activation seam
-    rbim::SweepRng rng;
-    rng.key = key;
-    rng.sweep = sweep;
-    rng.thr_any = thr > 0;
-    rng.thr_m1 = thr > 0 ? (uint32_t)min(thr - 1ull, 0xFFFFFFFFull) : 0u;
+    const rbim::SweepRng rng = rbim::make_rng(key, sweep, thr);
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     rbim::phase_activate_bonds<rbim::Word64>(t, rng, gt >> 5, nt >> 5);
 }

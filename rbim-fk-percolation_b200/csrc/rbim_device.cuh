@@ -24,8 +24,10 @@
 // loop with nonzero summed offset winds around the torus.  The loop sum of a
 // fundamental cycle is the winding number of a simple cycle, which is below L
 // in magnitude, so offsets may be stored modulo 2^k as long as L < 2^k:
-//   32-bit word: parent 16 bits | wx 8 bits | wy 8 bits   (N <= 65536, L <= 256)
-//   64-bit word: parent 32 bits | wx 16 bits | wy 16 bits (L <= 32768)
+//   Word64 (plain engine): parent 32 bits | wx 16 bits | wy 16 bits (L <= 32768)
+//   the resident engine labels the open lattice with 16-bit parents (no seam,
+//   so no offsets) and keeps offsets only for the roots that touch a seam
+//   (see rbim_resident.cu).
 // Parents always have a smaller index than their child (heads of runs, roots
 // hooked under smaller roots, path halving), so the structure is acyclic and
 // every root is the smallest site of its cluster, which makes labels canonical.
@@ -34,11 +36,14 @@
 //
 // Random numbers.  Philox4x32-10 (Salmon et al., SC'11) keyed by the 64-bit
 // chain key, counter {block, sweep_lo, sweep_hi, stream}:
-//   stream 0: bond k of sweep t uses word (k & 3) of block k >> 2
+//   stream 0: bond k of sweep t draws u = 16-bit halfword (k & 7) of block k >> 3
+//             (halfword h = bits 16*(h&1).. of word h >> 1)
+//   stream 3: the same halfword of block k >> 3 gives v
 //   stream 1: flip of the cluster rooted at r uses bit (r & 127) of block r >> 7
 //   stream 2: hot-start spin of site n uses bit (n & 127) of block n >> 7, sweep 0
-// A bond is occupied iff it is satisfied and its word is < thr, with
-// thr = floor((1 - exp(-2 beta)) * 2^32) computed on the host in double.
+// A bond is occupied iff it is satisfied and (u << 16 | v) < thr, with
+// thr = floor((1 - exp(-2 beta)) * 2^32) computed on the host in double; v is
+// only drawn when u == thr >> 16, so one block serves eight bonds.
 #pragma once
 
 #include <cstdint>
@@ -54,6 +59,7 @@ constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;
 constexpr uint32_t kStreamBond = 0u;
 constexpr uint32_t kStreamFlip = 1u;
 constexpr uint32_t kStreamInit = 2u;
+constexpr uint32_t kStreamBondLow = 3u;
 
 // Error bits written to the status word.
 constexpr int kErrFindCap = 1;
@@ -191,22 +197,6 @@ __device__ __forceinline__ uint32_t ynext_word(const Ld &ld, uint32_t w, const G
 // ---------------------------------------------------------------------------
 // Union-find word traits.
 // ---------------------------------------------------------------------------
-struct Word32 {
-    using T = uint32_t;
-    static constexpr int kOffBits = 8;
-    static constexpr int kCountShift = 16;
-    __device__ __forceinline__ static uint32_t parent(T w) { return w & 0xFFFFu; }
-    __device__ __forceinline__ static int ox(T w) { return (int)(int8_t)(w >> 16); }
-    __device__ __forceinline__ static int oy(T w) { return (int)(int8_t)(w >> 24); }
-    __device__ __forceinline__ static T make(uint32_t p, int x, int y)
-    {
-        return (p & 0xFFFFu) | ((uint32_t)(x & 0xFF) << 16) | ((uint32_t)(y & 0xFF) << 24);
-    }
-    __device__ __forceinline__ static bool nonzero(int v) { return (int8_t)v != 0; }
-    __device__ __forceinline__ static uint32_t count(T w) { return w >> 16; }
-    __device__ __forceinline__ static T count_inc(uint32_t c) { return c << 16; }
-};
-
 struct Word64 {
     using T = unsigned long long;
     static constexpr int kOffBits = 16;
@@ -222,6 +212,16 @@ struct Word64 {
     __device__ __forceinline__ static T count_inc(uint32_t c) { return (T)c << 32; }
 };
 
+__device__ __forceinline__ void uf_atomic_add(unsigned long long *p, unsigned long long v) { atomicAdd(p, v); }
+__device__ __forceinline__ void uf_atomic_add(unsigned int *p, unsigned int v) { atomicAdd(p, v); }
+// 16-bit add through the aligned 32-bit container; the caller guarantees the
+// half does not overflow.
+__device__ __forceinline__ void uf_atomic_add(unsigned short *p, unsigned short v)
+{
+    const uintptr_t a = (uintptr_t)p;
+    atomicAdd((unsigned int *)(a & ~uintptr_t(3)), (unsigned int)v << (8u * (unsigned)(a & 2u)));
+}
+
 // Storage for one lattice's union-find words: a base pointer into shared or
 // global memory (generic addressing covers both).
 template <class WT>
@@ -231,7 +231,7 @@ struct UF {
     __device__ __forceinline__ T ld(uint32_t i) const { return *((volatile T *)(w + i)); }
     __device__ __forceinline__ void st(uint32_t i, T v) const { *((volatile T *)(w + i)) = v; }
     __device__ __forceinline__ T cas(uint32_t i, T expect, T v) const { return atomicCAS(w + i, expect, v); }
-    __device__ __forceinline__ void add(uint32_t i, T v) const { atomicAdd(w + i, v); }
+    __device__ __forceinline__ void add(uint32_t i, T v) const { uf_atomic_add(w + i, v); }
 };
 
 struct Plane {

@@ -12,8 +12,8 @@ namespace rbim {
 // Shared-memory layout of the resident engine for lattices of up to n_max
 // sites (n_max <= 65536).
 struct ResidentLayout {
-    uint32_t n_max, nw_max, l_max;
-    size_t off_uf, off_S, off_JH, off_JV, off_OH, off_OV, off_FLIP, off_ROOT, off_SEAMV, bytes;
+    uint32_t n_max, nw_max, l_max, hs;
+    size_t off_uf, off_S, off_JH, off_JV, off_OH, off_OV, off_FLIP, off_ROOT, off_SEAMV, off_HK, off_HW, bytes;
 };
 
 ResidentLayout resident_layout(uint32_t l_max, int threads);

@@ -37,23 +37,55 @@ struct Lat {
 struct SweepRng {
     uint64_t key;
     uint64_t sweep;
-    uint32_t thr_m1;  // threshold - 1 (valid when thr_any)
-    bool thr_any;     // threshold > 0
+    uint32_t thr_hi;  // threshold >> 16
+    uint32_t thr_lo;  // threshold & 0xFFFF
+    bool thr_all;     // threshold == 2^32: every satisfied bond is occupied
 };
 
-// (a) Bond activation.  Items are 64-site chunks; lane i of the warp owning
-// chunk c draws Philox block 32c + i, which holds the four bonds of sites
-// 64c + 2i and 64c + 2i + 1.  SEAMV must be zero on entry.
+__device__ __forceinline__ SweepRng make_rng(uint64_t key, uint64_t sweep, uint64_t thr)
+{
+    SweepRng r;
+    r.key = key;
+    r.sweep = sweep;
+    r.thr_all = thr >= (1ull << 32);
+    r.thr_hi = (uint32_t)(thr >> 16) & 0xFFFFu;
+    r.thr_lo = (uint32_t)thr & 0xFFFFu;
+    return r;
+}
+
+// Spread the low 8 bits of v to bit positions 0, 4, 8, ..., 28.
+__device__ __forceinline__ uint32_t spread8x4(uint32_t v)
+{
+    v &= 0xFFu;
+    v = (v | (v << 12)) & 0x000F000Fu;
+    v = (v | (v << 6)) & 0x03030303u;
+    v = (v | (v << 3)) & 0x11111111u;
+    return v;
+}
+
+// Occupation decision of one bond from its 16-bit draw u: u < thr_hi
+// accepts, u > thr_hi rejects, u == thr_hi (probability 2^-16) defers to the
+// low half v, drawn separately.  Returns 0 reject, 1 accept, 2 undecided.
+__device__ __forceinline__ uint32_t bond_decide(const SweepRng &rng, uint32_t u)
+{
+    if (rng.thr_all || u < rng.thr_hi) return 1u;
+    return u == rng.thr_hi ? 2u : 0u;
+}
+
+// (a) Bond activation.  Items are 128-site chunks (four plane words); lane i
+// of the warp owning chunk c draws Philox block 32c + i, whose word s holds
+// the 16-bit draws of the horizontal (low half) and vertical (high half) bond
+// of site 128c + 4i + s.  SEAMV must be zero on entry.
 template <class WT>
 __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const SweepRng &rng, uint32_t warp,
                                                      uint32_t nwarps)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
-    const uint32_t nchunks = (g.N + 63u) >> 6;
+    const uint32_t nchunks = (g.N + 127u) >> 7;
     Plane S{t.S};
     for (uint32_t c = warp; c < nchunks; c += nwarps) {
-        const uint32_t wl = 2u * c + (lane >> 4);
+        const uint32_t wl = 4u * c + (lane >> 3);
         uint32_t sh = 0, sv = 0;
         if (wl < g.NW) {
             const uint32_t v = g.valid(wl);
@@ -61,25 +93,47 @@ __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const Swe
             sh = ~(s ^ xnext_word(S, wl, g) ^ t.JH[wl]) & v;
             sv = ~(s ^ ynext_word(S, wl, g) ^ t.JV[wl]) & v;
         }
+        const uint32_t sb = 4u * (lane & 7u);
+        sh = (sh >> sb) & 0xFu;  // satisfied bits of this lane's four sites
+        sv = (sv >> sb) & 0xFu;
         const U4 r = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBond);
-        const uint32_t be = 2u * (lane & 15u);
-        const bool he = ((sh >> be) & 1u) && rng.thr_any && r.x <= rng.thr_m1;
-        const bool ve = ((sv >> be) & 1u) && rng.thr_any && r.y <= rng.thr_m1;
-        const bool ho = ((sh >> (be + 1u)) & 1u) && rng.thr_any && r.z <= rng.thr_m1;
-        const bool vo = ((sv >> (be + 1u)) & 1u) && rng.thr_any && r.w <= rng.thr_m1;
-        const uint32_t eh = __ballot_sync(0xFFFFFFFFu, he), oh = __ballot_sync(0xFFFFFFFFu, ho);
-        const uint32_t ev = __ballot_sync(0xFFFFFFFFu, ve), ov = __ballot_sync(0xFFFFFFFFu, vo);
-        if (lane < 4u) {
-            const uint32_t hi = lane & 1u;  // 0: word 2c, 1: word 2c+1
-            const uint32_t w = 2u * c + hi;
+        uint32_t dh[4], dv[4];
+        bool refine = false;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t w = u4_word(r, s);
+            dh[s] = ((sh >> s) & 1u) ? bond_decide(rng, w & 0xFFFFu) : 0u;
+            dv[s] = ((sv >> s) & 1u) ? bond_decide(rng, w >> 16) : 0u;
+            refine |= (dh[s] == 2u) | (dv[s] == 2u);
+        }
+        if (refine) {
+            const U4 q = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBondLow);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t w = u4_word(q, s);
+                if (dh[s] == 2u) dh[s] = (w & 0xFFFFu) < rng.thr_lo ? 1u : 0u;
+                if (dv[s] == 2u) dv[s] = (w >> 16) < rng.thr_lo ? 1u : 0u;
+            }
+        }
+        uint32_t oh = 0, ov = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
+            const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
+            // Word j of the chunk collects lanes 8j .. 8j+7.
+            const uint32_t j = lane & 3u;
+            oh |= spread8x4(bh >> (8u * j)) << s;
+            ov |= spread8x4(bv >> (8u * j)) << s;
+        }
+        if (lane < 8u) {
+            const uint32_t w = 4u * c + (lane & 3u);
             if (w < g.NW) {
-                if (lane < 2u) {
-                    t.OH[w] = spread16(eh >> (16u * hi)) | (spread16(oh >> (16u * hi)) << 1);
+                if (lane < 4u) {
+                    t.OH[w] = oh;
                 } else {
-                    const uint32_t full = spread16(ev >> (16u * hi)) | (spread16(ov >> (16u * hi)) << 1);
                     const uint32_t re = g.row_end(w);
-                    t.OV[w] = full & ~re;
-                    uint32_t seam = full & re;
+                    t.OV[w] = ov & ~re;
+                    uint32_t seam = ov & re;
                     while (seam) {
                         const uint32_t b = __ffs(seam) - 1u;
                         seam &= seam - 1u;

@@ -152,11 +152,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_activate(PlainArgs a)
 {
     if (!chain_phase(a.chain)) return;
     const Lat<Word64> t = plain_lat(a);
-    SweepRng rng;
-    rng.key = a.chain->key;
-    rng.sweep = a.chain->sweep;
-    rng.thr_any = a.chain->thr > 0;
-    rng.thr_m1 = a.chain->thr > 0 ? (uint32_t)min(a.chain->thr - 1ull, 0xFFFFFFFFull) : 0u;
+    const SweepRng rng = make_rng(a.chain->key, a.chain->sweep, a.chain->thr);
     phase_activate<Word64>(t, rng, gwarp(), gnwarps(), gtid(), gnthreads());
 }
 

@@ -1,9 +1,20 @@
 // Resident engine: one lattice per CTA, held in shared memory for every sweep
 // of a call.  A persistent grid pulls chains from a work queue (an atomic
-// counter in global memory), loads the chain's spin and coupling planes,
-// runs its sweeps entirely on chip (bond activation, run-based union-find with
-// image offsets for exact wrapping, flip, measurement) and writes back only
-// the spin plane, the bin sums and the optional per-sweep records.
+// counter in global memory), loads the chain's spin and coupling planes, runs
+// its sweeps entirely on chip and writes back only the spin plane, the bin
+// sums and the optional per-sweep records.
+//
+// Labelling runs in two stages so that a whole L = 256 lattice fits one CTA:
+//  1. the open lattice (every bond except the 2L that close the periodic
+//     boundary) is labelled with a union-find of 16-bit parents: inside the
+//     open rectangle every cycle is contractible, so no image offsets are
+//     needed and each open cluster's root is its smallest site;
+//  2. the roots of the open clusters that touch a seam bond are hashed into a
+//     small table whose union-find words carry image offsets; the seam bonds
+//     are unioned there, and a seam bond that closes a loop with nonzero
+//     summed offset winds around the torus (the exact test of the reference,
+//     src/rbim/_unionfind.py:104-124).  Each merged open root is then pointed
+//     at the smallest open root of its full cluster.
 //
 // This replaces, per chain, the loop of run_single_realization
 // (src/rbim/simulation.py:196-242) around sw_sweep
@@ -17,25 +28,60 @@ namespace rbim {
 
 namespace {
 
-constexpr uint32_t kMaxResidentSites = 65536;  // 16-bit parents in Word32
+constexpr uint32_t kMaxResidentSites = 65536;  // 16-bit parents
 // Dynamic shared memory budget: the 227 KB per-CTA limit minus room for the
 // kernels' static shared scratch.
 constexpr size_t kMaxSmem = 227 * 1024 - 8 * 1024;
+constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 
 size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
+uint32_t hash_size(uint32_t l_max)
+{
+    // At most 4L distinct open roots touch a seam bond; keep the load <= 1/2.
+    uint32_t h = 32;
+    while (h < 8u * l_max) h *= 2;
+    return h;
+}
+
 }  // namespace
+
+// Open-lattice union-find word: the parent site only.
+struct Word16 {
+    using T = unsigned short;
+    __device__ __forceinline__ static uint32_t parent(T w) { return w; }
+    __device__ __forceinline__ static int ox(T) { return 0; }
+    __device__ __forceinline__ static int oy(T) { return 0; }
+    __device__ __forceinline__ static T make(uint32_t p, int, int) { return (T)p; }
+    __device__ __forceinline__ static T count_inc(uint32_t c) { return (T)c; }
+};
+
+// Seam union-find word: parent slot (12 bits) | wx (10 bits) | wy (10 bits),
+// offsets modulo 1024 (exact for L < 1024, see rbim_device.cuh).
+struct SeamWord {
+    using T = uint32_t;
+    __device__ __forceinline__ static uint32_t parent(T w) { return w & 0xFFFu; }
+    __device__ __forceinline__ static int ox(T w) { return ((int)(w << 10)) >> 22; }
+    __device__ __forceinline__ static int oy(T w) { return ((int)w) >> 22; }
+    __device__ __forceinline__ static T make(uint32_t p, int x, int y)
+    {
+        return (p & 0xFFFu) | ((uint32_t)(x & 0x3FF) << 12) | ((uint32_t)(y & 0x3FF) << 22);
+    }
+    __device__ __forceinline__ static bool nonzero(int v) { return (v & 0x3FF) != 0; }
+};
 
 ResidentLayout resident_layout(uint32_t l_max, int threads)
 {
+    (void)threads;
     ResidentLayout ly{};
     ly.l_max = l_max;
     ly.n_max = l_max * l_max;
     const uint32_t nw = (ly.n_max + 31u) / 32u;
     ly.nw_max = (nw + 3u) & ~3u;
+    ly.hs = hash_size(l_max);
     size_t off = 0;
     ly.off_uf = off;
-    off = align16(off + 4ull * ly.n_max);
+    off = align16(off + 2ull * ly.n_max);
     const size_t plane = 4ull * (ly.nw_max + 4u);
     ly.off_S = off;
     off += plane;
@@ -53,8 +99,11 @@ ResidentLayout resident_layout(uint32_t l_max, int threads)
     off += plane;
     ly.off_SEAMV = off;
     off = align16(off + 4ull * (((l_max + 31u) / 32u) + 4u));
-    ly.bytes = off;
-    (void)threads;
+    ly.off_HK = off;
+    off += 4ull * ly.hs;
+    ly.off_HW = off;
+    off += 4ull * ly.hs;
+    ly.bytes = align16(off);
     return ly;
 }
 
@@ -98,13 +147,21 @@ struct MinBlocks {
     static constexpr int value = NT >= 1024 ? 1 : 1024 / NT;
 };
 
+// Per-CTA view of the shared-memory arrays of one lattice.
+struct Res {
+    Lat<Word16> t;
+    uint32_t *HK;  // seam hash keys: open root site, or kHashEmpty
+    uint32_t *HW;  // seam union-find words (SeamWord)
+    uint32_t hs, hs_log2;
+};
+
 template <int NT>
-__device__ __forceinline__ Lat<Word32> make_lat(unsigned char *smem, const ResidentLayout &ly, uint32_t L,
-                                                Red<NT> &red)
+__device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayout &ly, uint32_t L, Red<NT> &red)
 {
-    Lat<Word32> t;
+    Res r;
+    Lat<Word16> &t = r.t;
     t.g = Geom{L, L * L, (L * L + 31u) / 32u};
-    t.uf.w = (uint32_t *)(smem + ly.off_uf);
+    t.uf.w = (unsigned short *)(smem + ly.off_uf);
     t.S = (uint32_t *)(smem + ly.off_S);
     t.JH = (const uint32_t *)(smem + ly.off_JH);
     t.JV = (const uint32_t *)(smem + ly.off_JV);
@@ -116,52 +173,227 @@ __device__ __forceinline__ Lat<Word32> make_lat(unsigned char *smem, const Resid
     t.wrap = &red.wrap;
     t.err = &red.err;
     t.cap = t.g.N + 64u;
-    return t;
+    r.HK = (uint32_t *)(smem + ly.off_HK);
+    r.HW = (uint32_t *)(smem + ly.off_HW);
+    r.hs = ly.hs;
+    r.hs_log2 = 31u - __clz(ly.hs);
+    return r;
 }
 
-// Measurement of one sweep after phase_finalize(count = true): energy,
-// magnetization, n_clusters, S1, S2, |M_C1| (reference sw_sweep,
+// Mask of the bits of word w whose site lies in the last row (x = L-1): the
+// horizontal bonds there close the x boundary.
+__device__ __forceinline__ uint32_t last_row_mask(const Geom &g, uint32_t w)
+{
+    const uint32_t n0 = w << 5, first = g.N - g.L;
+    if (n0 + 32u <= first) return 0u;
+    const uint32_t v = g.valid(w);
+    if (n0 >= first) return v;
+    return ~((1u << (first - n0)) - 1u) & v;
+}
+
+// Open-lattice union: hook the larger root under the smaller with a 16-bit CAS.
+__device__ __forceinline__ void union_open(const UF<Word16> &uf, uint32_t a, uint32_t b, uint32_t cap, int *err)
+{
+    for (uint32_t it = 0; it < cap; ++it) {
+        a = uf_root<Word16>(uf, a, cap, err);
+        b = uf_root<Word16>(uf, b, cap, err);
+        if (a == b) return;
+        if (a > b) {
+            const uint32_t x = a;
+            a = b;
+            b = x;
+        }
+        if (uf.cas(b, (unsigned short)b, (unsigned short)a) == (unsigned short)b) return;
+    }
+    atomicOr(err, kErrUnionCap);
+}
+
+// (b) Open-lattice unions across occupied x-bonds that do not cross the x
+// seam; the plaquette rule of phase_union skips bonds already connected.
+__device__ __forceinline__ void phase_union_open(const Lat<Word16> &t, uint32_t warp, uint32_t nwarps)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const Geom &g = t.g;
+    Plane OVp{t.OV};
+    for (uint32_t w = warp; w < g.NW; w += nwarps) {
+        const uint32_t oh = t.OH[w] & ~last_row_mask(g, w);
+        if (!oh) continue;
+        const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
+        const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
+        const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
+        const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
+        const uint32_t prev_ovx = extract32(OVp, ((w << 5) + g.L - 1u) % g.N, g);
+        const uint32_t need = oh & ~(prev_oh & prev_ov & prev_ovx);
+        if ((need >> lane) & 1u) {
+            const uint32_t n = (w << 5) + lane;
+            union_open(t.uf, n, n + g.L, t.cap, t.err);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t hash_insert(const Res &r, uint32_t key, int *err)
+{
+    uint32_t h = (key * 0x9E3779B1u) >> (32u - r.hs_log2);
+    for (uint32_t it = 0; it < r.hs; ++it) {
+        const uint32_t old = atomicCAS(r.HK + h, kHashEmpty, key);
+        if (old == kHashEmpty || old == key) return h;
+        h = (h + 1u) & (r.hs - 1u);
+    }
+    atomicOr(err, kErrUnionCap);
+    return 0;
+}
+
+// Union of two seam nodes across a seam bond with seam crossing (ex, ey); the
+// node whose open root is larger is hooked under the other.
+__device__ __forceinline__ void seam_union(const Res &r, uint32_t na, uint32_t nb, int ex, int ey, int *wrap,
+                                           uint32_t cap, int *err)
+{
+    const UF<SeamWord> hw{r.HW};
+    for (uint32_t it = 0; it < cap; ++it) {
+        const FindResult fa = uf_find<SeamWord>(hw, na, cap, err);
+        const FindResult fb = uf_find<SeamWord>(hw, nb, cap, err);
+        if (fa.root == fb.root) {
+            int f = 0;
+            if (SeamWord::nonzero(ex + fb.ax - fa.ax)) f |= 1;
+            if (SeamWord::nonzero(ey + fb.ay - fa.ay)) f |= 2;
+            if (f) atomicOr(wrap, f);
+            return;
+        }
+        const uint32_t ka = r.HK[fa.root], kb = r.HK[fb.root];
+        if (ka < kb) {
+            const uint32_t expect = SeamWord::make(fb.root, 0, 0);
+            if (hw.cas(fb.root, expect, SeamWord::make(fa.root, fa.ax - ex - fb.ax, fa.ay - ey - fb.ay)) == expect)
+                return;
+        } else {
+            const uint32_t expect = SeamWord::make(fa.root, 0, 0);
+            if (hw.cas(fa.root, expect, SeamWord::make(fb.root, fb.ax + ex - fa.ax, fb.ay + ey - fa.ay)) == expect)
+                return;
+        }
+    }
+    atomicOr(err, kErrUnionCap);
+}
+
+// Seam table reset (before the seam phase).
+__device__ __forceinline__ void seam_reset(const Res &r, uint32_t tid, uint32_t nthreads)
+{
+    for (uint32_t k = tid; k < r.hs; k += nthreads) {
+        r.HK[k] = kHashEmpty;
+        r.HW[k] = SeamWord::make(k, 0, 0);
+    }
+}
+
+// (b) Seam bonds: x seam (x = L-1 -> 0, crossing (1,0)) and y seam
+// (y = L-1 -> 0, crossing (0,1)).  The open union-find is final here.
+__device__ __forceinline__ void phase_seam(const Res &r, uint32_t tid, uint32_t nthreads)
+{
+    const Lat<Word16> &t = r.t;
+    const Geom &g = t.g;
+    for (uint32_t i = tid; i < 2u * g.L; i += nthreads) {
+        uint32_t a, b;
+        int ex, ey;
+        if (i < g.L) {
+            a = g.N - g.L + i;
+            if (!((t.OH[a >> 5] >> (a & 31u)) & 1u)) continue;
+            b = i;
+            ex = 1;
+            ey = 0;
+        } else {
+            const uint32_t x = i - g.L;
+            if (!((t.SEAMV[x >> 5] >> (x & 31u)) & 1u)) continue;
+            a = x * g.L + g.L - 1u;
+            b = x * g.L;
+            ex = 0;
+            ey = 1;
+        }
+        const uint32_t ra = uf_root_ro<Word16>(t.uf, a, t.cap, t.err);
+        const uint32_t rb = uf_root_ro<Word16>(t.uf, b, t.cap, t.err);
+        const uint32_t na = hash_insert(r, ra, t.err);
+        const uint32_t nb = hash_insert(r, rb, t.err);
+        seam_union(r, na, nb, ex, ey, t.wrap, t.cap, t.err);
+    }
+}
+
+// (b) Point every merged open root at the smallest open root of its cluster.
+__device__ __forceinline__ void phase_seam_propagate(const Res &r, uint32_t tid, uint32_t nthreads)
+{
+    const UF<SeamWord> hw{r.HW};
+    for (uint32_t k = tid; k < r.hs; k += nthreads) {
+        const uint32_t key = r.HK[k];
+        if (key == kHashEmpty) continue;
+        const uint32_t g = uf_root_ro<SeamWord>(hw, k, r.hs + 1u, r.t.err);
+        if (g != k) r.t.uf.st(key, (unsigned short)r.HK[g]);
+    }
+}
+
+// The labelling stages shared by the sweep and label kernels, from occupied
+// bond planes to final roots; barriers between stages.  Returns the number of
+// roots counted by this warp.
+template <int NT>
+__device__ __forceinline__ uint32_t resident_label(const Res &r, bool flip)
+{
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    constexpr uint32_t nwarps = NT / 32;
+    phase_heads<Word16>(r.t, warp, nwarps);
+    seam_reset(r, tid, NT);
+    __syncthreads();
+    phase_union_open(r.t, warp, nwarps);
+    __syncthreads();
+    phase_seam(r, tid, NT);
+    __syncthreads();
+    phase_seam_propagate(r, tid, NT);
+    for (uint32_t i = tid; i < (r.t.g.L + 31u) / 32u; i += NT) r.t.SEAMV[i] = 0u;
+    __syncthreads();
+    const uint32_t nr = phase_finalize<Word16>(r.t, warp, nwarps, flip, false);
+    __syncthreads();
+    return nr;
+}
+
+// Add v to the 16-bit word i through its 32-bit container (no carry can
+// leave the half: cluster sizes stay below 65536 whenever counts are taken).
+__device__ __forceinline__ void add16(unsigned short *base, uint32_t i, uint32_t v)
+{
+    atomicAdd((unsigned int *)(base + (i & ~1u)), v << (16u * (i & 1u)));
+}
+
+// Measurement of one sweep after resident_label: energy, magnetization,
+// n_clusters, S1, S2, |M_C1| (reference sw_sweep,
 // src/rbim/swendsen_wang.py:146-172).  Ends with a barrier.  Thread 0 returns
 // the record in rec.
 template <int NT>
-__device__ __forceinline__ void resident_measure(const Lat<Word32> &t, Red<NT> &red, uint32_t nroots_warp,
+__device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, uint32_t nroots_warp,
                                                  long long rec[kRecLen])
 {
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     constexpr uint32_t nwarps = NT / 32;
+    const Lat<Word16> &t = res.t;
     const Geom &g = t.g;
+    unsigned short *u16 = t.uf.w;
+
+    // Energy and magnetization of the flipped spins; root counters to zero.
     uint32_t unsat = 0, downs = 0;
     measure_energy(g, t.S, t.JH, t.JV, tid, NT, unsat, downs);
-    uint32_t k1 = 0, k2 = 0;
     for (uint32_t w = tid; w < g.NW; w += NT) {
         uint32_t roots = t.ROOT[w];
         while (roots) {
             const uint32_t b = __ffs(roots) - 1u;
             roots &= roots - 1u;
-            const uint32_t r = (w << 5) + b;
-            const uint32_t key = (Word32::count(t.uf.ld(r)) << 16) | (0xFFFFu - r);
-            top2_merge(k1, k2, key, 0u);
+            u16[(w << 5) + b] = 0;
         }
     }
-    warp_top2(k1, k2);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         unsat += __shfl_xor_sync(0xFFFFFFFFu, unsat, o);
         downs += __shfl_xor_sync(0xFFFFFFFFu, downs, o);
     }
     if (lane == 0) {
-        red.k1[warp] = k1;
-        red.k2[warp] = k2;
         red.unsat[warp] = unsat;
         red.downs[warp] = downs;
         red.roots[warp] = nroots_warp;
     }
     __syncthreads();
     if (warp == 0) {
-        uint32_t a1 = lane < nwarps ? red.k1[lane] : 0u, a2 = lane < nwarps ? red.k2[lane] : 0u;
         uint32_t u = lane < nwarps ? red.unsat[lane] : 0u, d = lane < nwarps ? red.downs[lane] : 0u;
         uint32_t nr = lane < nwarps ? red.roots[lane] : 0u;
-        warp_top2(a1, a2);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             u += __shfl_xor_sync(0xFFFFFFFFu, u, o);
@@ -172,41 +404,73 @@ __device__ __forceinline__ void resident_measure(const Lat<Word32> &t, Red<NT> &
             red.ncl = nr;
             red.unsat_t = u;
             red.downs_t = d;
-            if (nr == 1) {
-                // One cluster covers the lattice (its 16-bit size field may
-                // have wrapped at N = 65536).
-                red.g1 = 0;
-                red.s1 = g.N;
-                red.s2 = 0;
-            } else {
+        }
+    }
+    // Cluster sizes into the root words (warp-aggregated per root).
+    for (uint32_t w = warp; w < g.NW; w += nwarps) {
+        const uint32_t n = (w << 5) + lane;
+        const bool ok = n < g.N;
+        uint32_t r = 0;
+        if (ok) r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
+        const uint32_t live = __ballot_sync(0xFFFFFFFFu, ok);
+        if (ok) {
+            const uint32_t grp = __match_any_sync(live, r);
+            if (lane == (uint32_t)(__ffs(grp) - 1)) add16(u16, r, __popc(grp));
+        }
+    }
+    __syncthreads();
+    const uint32_t ncl = red.ncl;
+    if (ncl > 1) {
+        uint32_t k1 = 0, k2 = 0;
+        for (uint32_t w = tid; w < g.NW; w += NT) {
+            uint32_t roots = t.ROOT[w];
+            while (roots) {
+                const uint32_t b = __ffs(roots) - 1u;
+                roots &= roots - 1u;
+                const uint32_t r = (w << 5) + b;
+                top2_merge(k1, k2, ((uint32_t)u16[r] << 16) | (0xFFFFu - r), 0u);
+            }
+        }
+        warp_top2(k1, k2);
+        if (lane == 0) {
+            red.k1[warp] = k1;
+            red.k2[warp] = k2;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t a1 = lane < nwarps ? red.k1[lane] : 0u, a2 = lane < nwarps ? red.k2[lane] : 0u;
+            warp_top2(a1, a2);
+            if (lane == 0) {
                 red.g1 = 0xFFFFu - (a1 & 0xFFFFu);
                 red.s1 = a1 >> 16;
                 red.s2 = a2 >> 16;
             }
         }
-    }
-    __syncthreads();
-    const uint32_t ncl = red.ncl;
-    const long long M = (long long)g.N - 2ll * (long long)red.downs_t;
-    long long mc_total;
-    if (ncl > 1) {
+        __syncthreads();
         const uint32_t g1 = red.g1;
         int mc = 0;
         for (uint32_t w = warp; w < g.NW; w += nwarps) {
             const uint32_t n = (w << 5) + lane;
-            const bool in = n < g.N && Word32::parent(t.uf.ld(n)) == g1;
+            const bool root = (t.ROOT[w] >> lane) & 1u;
+            const bool in = n < g.N && (root ? n == g1 : (uint32_t)u16[n] == g1);
             const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
             if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
         }
         if (lane == 0) red.mc[warp] = mc;
         __syncthreads();
-        mc_total = 0;
-        if (tid == 0)
-            for (uint32_t i = 0; i < nwarps; ++i) mc_total += red.mc[i];
-    } else {
-        mc_total = M;
+    } else if (tid == 0) {
+        // One cluster covers the lattice.
+        red.g1 = 0;
+        red.s1 = g.N;
+        red.s2 = 0;
     }
+    const long long M = (long long)g.N - 2ll * (long long)red.downs_t;
     if (tid == 0) {
+        long long mc_total = M;
+        if (ncl > 1) {
+            mc_total = 0;
+            for (uint32_t i = 0; i < nwarps; ++i) mc_total += red.mc[i];
+        }
         rec[0] = 2ll * (long long)red.unsat_t - 2ll * (long long)g.N;
         rec[1] = M;
         rec[2] = ncl;
@@ -220,10 +484,10 @@ __device__ __forceinline__ void resident_measure(const Lat<Word32> &t, Red<NT> &
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool,
-                                                        const uint32_t *coupling_pool, long long *acc_i,
-                                                        double *acc_f, int32_t *records, int n_sweeps, int *queue,
-                                                        int *status, ResidentLayout ly)
+__global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
+    k_resident_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                      long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *queue, int *status,
+                      ResidentLayout ly)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Red<NT> red;
@@ -232,16 +496,16 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_sweeps(rb
 
     if (tid == 0) red.err = 0;
     for (;;) {
-        if (tid == 0) red.item = atomicAdd(queue, 1);
+        if (tid == 0) {
+            red.item = atomicAdd(queue, 1);
+            if (red.item < n_chains) {
+                red.ch = chains[red.item];
+                red.cur_bin = -1;
+            }
+        }
         __syncthreads();
         const int item = red.item;
         if (item >= n_chains) break;
-        if (tid == 0) {
-            red.ch = chains[item];
-            red.acc.zero();
-            red.cur_bin = -1;
-        }
-        __syncthreads();
         const rbim_chain_t &ch = red.ch;
         if (ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 || ch.n_therm < 0) {
             if (tid == 0) atomicOr(status, kErrBadChain);
@@ -249,7 +513,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_sweeps(rb
             continue;
         }
         const uint32_t L = (uint32_t)ch.L;
-        Lat<Word32> t = make_lat<NT>(smem, ly, L, red);
+        const Res res = make_res<NT>(smem, ly, L, red);
+        const Lat<Word16> &t = res.t;
         const Geom g = t.g;
         const uint32_t nwp = (g.NW + 3u) & ~3u;
 
@@ -268,28 +533,17 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_sweeps(rb
         const uint64_t t_end = (uint64_t)ch.n_therm + (uint64_t)ch.n_bins * (uint64_t)ch.sweeps_per_bin;
         uint64_t sweep = ch.sweep;
         const uint64_t stop = min(t_end, sweep + (uint64_t)max(n_sweeps, 0));
-        SweepRng rng;
-        rng.key = ch.key;
-        rng.thr_any = ch.thr > 0;
-        rng.thr_m1 = ch.thr > 0 ? (uint32_t)min(ch.thr - 1ull, 0xFFFFFFFFull) : 0u;
         __syncthreads();
 
         for (; sweep < stop; ++sweep) {
             const bool measure = sweep >= (uint64_t)ch.n_therm;
-            rng.sweep = sweep;
             if (tid == 0) red.wrap = 0;
-            phase_activate<Word32>(t, rng, warp, nwarps, tid, NT);
+            phase_activate<Word16>(t, make_rng(ch.key, sweep, ch.thr), warp, nwarps, tid, NT);
             __syncthreads();
-            phase_heads<Word32>(t, warp, nwarps);
-            __syncthreads();
-            phase_union<Word32>(t, warp, nwarps, tid, NT);
-            __syncthreads();
-            const uint32_t nr = phase_finalize<Word32>(t, warp, nwarps, true, measure);
-            for (uint32_t i = tid; i < (L + 31u) / 32u; i += NT) t.SEAMV[i] = 0u;
-            __syncthreads();
+            const uint32_t nr = resident_label<NT>(res, true);
             if (measure) {
                 long long rec[kRecLen];
-                resident_measure<NT>(t, red, nr, rec);
+                resident_measure<NT>(res, red, nr, rec);
                 if (tid == 0) {
                     const long long idx = (long long)(sweep - (uint64_t)ch.n_therm);
                     const long long bin = idx / ch.sweeps_per_bin;
@@ -329,21 +583,21 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_sweeps(rb
 
 // Labelling only: frozen occupation bytes in, canonical labels out.
 template <int NT>
-__global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_label(uint32_t L, const uint8_t *occ, int32_t *labels,
-                                                       int32_t *n_clusters, uint8_t *wraps, int *status,
-                                                       ResidentLayout ly)
+__global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
+    k_resident_label(uint32_t L, const uint8_t *occ, int32_t *labels, int32_t *n_clusters, uint8_t *wraps,
+                     int *status, ResidentLayout ly)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Red<NT> red;
     __shared__ uint32_t s_scan[NT];
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    constexpr uint32_t nwarps = NT / 32;
+    const uint32_t tid = threadIdx.x;
     const size_t lat = blockIdx.x;
     if (tid == 0) {
         red.err = 0;
         red.wrap = 0;
     }
-    Lat<Word32> t = make_lat<NT>(smem, ly, L, red);
+    const Res res = make_res<NT>(smem, ly, L, red);
+    const Lat<Word16> &t = res.t;
     const Geom g = t.g;
     const uint8_t *o = occ + lat * 2ull * g.N;
     for (uint32_t i = tid; i < (L + 31u) / 32u; i += NT) t.SEAMV[i] = 0u;
@@ -368,13 +622,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_label(uin
         }
     }
     __syncthreads();
-    phase_heads<Word32>(t, warp, nwarps);
-    __syncthreads();
-    phase_union<Word32>(t, warp, nwarps, tid, NT);
-    __syncthreads();
-    const uint32_t nr = phase_finalize<Word32>(t, warp, nwarps, false, false);
-    if (lane == 0) red.roots[warp] = nr;
-    __syncthreads();
+    resident_label<NT>(res, false);
     // Exclusive prefix of root counts over words -> FLIP plane (rank base).
     const uint32_t per = (g.NW + NT - 1u) / NT;
     const uint32_t w0 = tid * per, w1 = min(g.NW, w0 + per);
@@ -396,7 +644,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value) k_resident_label(uin
     __syncthreads();
     int32_t *lab = labels + lat * (size_t)g.N;
     for (uint32_t n = tid; n < g.N; n += NT) {
-        const uint32_t r = Word32::parent(t.uf.ld(n));
+        const uint32_t r = Word16::parent(t.uf.ld(n));
         lab[n] = (int32_t)(t.FLIP[r >> 5] + __popc(t.ROOT[r >> 5] & ((1u << (r & 31u)) - 1u)));
     }
     if (tid == 0) {

@@ -34,6 +34,39 @@ def test_activation_matches_philox_replay(rb, orc, L):
         assert np.array_equal(got, want), (L, T)
 
 
+def test_activation_refinement_branch(rb, orc):
+    """Thresholds whose high half equals a bond's 16-bit draw force the second-stream draw."""
+    L, key, sweep = 16, 0x5EED, 3
+    lattice = rb.build_lattice(L)
+    J = np.ones(2 * L * L, dtype=np.int8)
+    spins = np.ones(L * L, dtype=np.int8)  # every bond satisfied
+    lib = rb._native.lib()
+    for k in (0, 7, 8, 101, 2 * L * L - 1):
+        u = orc.bond_uniform(key, sweep, k) >> 16
+        for lo in (0, 0x7FFF, 0xFFFF):
+            thr = (u << 16) | lo
+            want = orc.activate(L, spins, J, key=key, thr=thr, sweep=sweep)
+            got = _activate_thr(rb, lib, L, spins, J, key, thr, sweep)
+            assert np.array_equal(got, want), (k, lo)
+            full = orc.bond_uniform(key, sweep, k)
+            assert bool(want[k]) == (full < thr)
+
+
+def _activate_thr(rb, lib, L, spins, J, key, thr, sweep):
+    import ctypes
+    import torch
+
+    s = torch.from_numpy(rb.packing.pack_spins(spins, L).view(np.int32)).cuda()
+    j = torch.from_numpy(rb.packing.pack_couplings(J, L).view(np.int32)).cuda()
+    occ = torch.empty(2 * L * L, dtype=torch.uint8, device="cuda")
+    ws = torch.empty(int(lib.rbim_activate_workspace_bytes(L)), dtype=torch.uint8, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    rc = lib.rbim_activate(L, p(s), p(j), key, thr, sweep, p(occ), p(ws), ws.numel(),
+                           ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    rb._native.check(rc, "rbim_activate")
+    return occ.cpu().numpy().astype(bool)
+
+
 def test_activation_limits(rb):
     """Reference ``tests/test_clusters.py:30-59``: beta = 0 activates nothing, beta = 50 everything satisfied."""
     L = 8

@@ -84,6 +84,24 @@ def test_activation_only_satisfied_and_limits(orc):
     assert np.array_equal(orc.activate(L, spins, J, key=1, thr=2**32, sweep=0), sat)
 
 
+def test_lazy_activation_equals_full_uniform_comparison(orc):
+    """The oracle's eight-bonds-per-block activation equals comparing each bond's 32-bit uniform with thr."""
+    L, key, sweep = 9, 4242, 11
+    rng = np.random.default_rng(3)
+    J = np.where(rng.random(2 * L * L) < 0.3, -1, 1).astype(np.int8)
+    spins = np.where(rng.random(L * L) < 0.5, -1, 1).astype(np.int8)
+    a = np.arange(2 * L * L) >> 1
+    x, y = a // L, a % L
+    b = np.where(np.arange(2 * L * L) % 2 == 0, ((x + 1) % L) * L + y, x * L + (y + 1) % L)
+    sat = J * spins[a] * spins[b] > 0
+    uni = np.array([orc.bond_uniform(key, sweep, k) for k in range(2 * L * L)], dtype=np.uint64)
+    thrs = [0, 1, 2**31, 2**32 - 1, 2**32]
+    thrs += [int(uni[k] >> 16 << 16) | lo for k in (0, 5, 77) for lo in (0, 0x8000, 0xFFFF)]
+    for thr in thrs:
+        want = sat & (uni < thr)
+        assert np.array_equal(orc.activate(L, spins, J, key=key, thr=thr, sweep=sweep), want), thr
+
+
 def test_chain_is_deterministic_and_binning_invariant(orc):
     L = 8
     J = np.ones(2 * L * L, dtype=np.int8)
