@@ -216,6 +216,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--chains", type=int, default=0, help="use only the first N chains (profiling runs)")
     args = ap.parse_args()
 
     L, ps, n_real, temps = workload(args.workload)
@@ -240,6 +241,8 @@ def main():
     S = args.sweeps_per_step
     n_total = (args.warmup + args.steps) * S + 1
     specs, couplings = build_chains(rb, L, ps, n_real, temps, args.seed + 1000 * rank, n_total)
+    if args.chains > 0:
+        specs = specs[: args.chains]
     cs = rb.ChainSet(specs, couplings, device=dev)
     cs.init_spins(hot=True)
     n_chains = len(specs)

@@ -25,10 +25,14 @@
  * 3", SC'11), so a whole chain can be replayed bit for bit:
  *
  *   key     = 64-bit chain key, low word key[0], high word key[1]
- *   bond k of sweep t   : 32-bit uniform (u << 16) | v, where u is 16-bit
- *                         halfword (k & 7) of Philox(ctr = {k >> 3, t_lo, t_hi, 0})
- *                         and v the same halfword of Philox(ctr = {k >> 3, t_lo,
- *                         t_hi, 3}); halfword h is bits 16*(h&1).. of word h>>1.
+ *   bond k of sweep t   : site n = k >> 1, direction d = k & 1 (0 horizontal,
+ *                         1 vertical).  Sites come in chunks of 128; site n is
+ *                         lane i = n & 31 of row s = (n >> 5) & 3 of chunk
+ *                         n >> 7, and uses Philox block
+ *                         b = 32 * (n >> 7) + i, word s, half d (low half for
+ *                         d = 0).  Its 32-bit uniform is (u << 16) | v, with u
+ *                         that half of Philox(ctr = {b, t_lo, t_hi, 0}) and v
+ *                         the same half of Philox(ctr = {b, t_lo, t_hi, 3}).
  *                         Occupied iff satisfied and uniform < thr, where
  *                         thr = floor(p_add * 2^32), p_add = -expm1(-2 beta).
  *                         (The engine draws v only when u == thr >> 16.)
@@ -94,14 +98,17 @@ static void philox_stream(uint64_t key, uint64_t block, uint64_t sweep, uint32_t
     orc_philox4x32_10(ctr, k, out);
 }
 
+static inline uint64_t bond_block(uint64_t site) { return ((site >> 7) << 5) | (site & 31); }
+
 uint32_t orc_bond_uniform(uint64_t key, uint64_t sweep, uint64_t bond)
 {
     uint32_t hi[4], lo[4];
-    philox_stream(key, bond >> 3, sweep, 0u, hi);
-    philox_stream(key, bond >> 3, sweep, 3u, lo);
-    const unsigned h = (unsigned)(bond & 7);
-    const uint32_t u = (hi[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
-    const uint32_t v = (lo[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
+    const uint64_t n = bond >> 1;
+    const unsigned s = (unsigned)((n >> 5) & 3), d = (unsigned)(bond & 1);
+    philox_stream(key, bond_block(n), sweep, 0u, hi);
+    philox_stream(key, bond_block(n), sweep, 3u, lo);
+    const uint32_t u = (hi[s] >> (16 * d)) & 0xFFFFu;
+    const uint32_t v = (lo[s] >> (16 * d)) & 0xFFFFu;
     return (u << 16) | v;
 }
 
@@ -138,38 +145,46 @@ static inline int64_t bond_end_b(int64_t L, int64_t k)
 /* Bond activation (clusters.py:48-79)                                       */
 /* ------------------------------------------------------------------------ */
 
-/* Bonds are taken eight at a time (one Philox block); the low halves come
- * from the second stream only when some satisfied bond's high half equals
- * thr >> 16, which yields the same decisions as comparing every bond's full
- * orc_bond_uniform with thr. */
+/* Bonds are taken eight at a time (one Philox block: the two bonds of the
+ * four sites 128c + 32s + i, s = 0..3); the low halves come from the second
+ * stream only when some satisfied bond's high half equals thr >> 16, which
+ * yields the same decisions as comparing every bond's full orc_bond_uniform
+ * with thr. */
 void orc_activate(int64_t L, const int8_t *spins, const int8_t *J, uint64_t key, uint64_t thr,
                   uint64_t sweep, uint8_t *occ)
 {
-    int64_t nb = 2 * L * L;
+    const int64_t n_sites = L * L;
     const uint32_t thr_hi = (uint32_t)(thr >> 16);
-    for (int64_t k0 = 0; k0 < nb; k0 += 8) {
-        uint32_t hi[4], lo[4];
-        int have_lo = 0;
-        philox_stream(key, (uint64_t)k0 >> 3, sweep, 0u, hi);
-        for (int64_t k = k0; k < k0 + 8 && k < nb; ++k) {
-            int64_t a = k >> 1, b = bond_end_b(L, k);
-            int satisfied = (int)J[k] * (int)spins[a] * (int)spins[b] > 0;
-            const unsigned h = (unsigned)(k & 7);
-            const uint32_t u = (hi[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
-            int on = 0;
-            if (satisfied) {
-                if (thr >= (1ull << 32) || u < thr_hi) {
-                    on = 1;
-                } else if (u == thr_hi) {
-                    if (!have_lo) {
-                        philox_stream(key, (uint64_t)k0 >> 3, sweep, 3u, lo);
-                        have_lo = 1;
+    for (int64_t c = 0; c * 128 < n_sites; ++c) {
+        for (int64_t i = 0; i < 32; ++i) {
+            uint32_t hi[4], lo[4];
+            int have_lo = 0;
+            philox_stream(key, (uint64_t)(32 * c + i), sweep, 0u, hi);
+            for (int s = 0; s < 4; ++s) {
+                const int64_t n = 128 * c + 32 * s + i;
+                if (n >= n_sites)
+                    continue;
+                for (int d = 0; d < 2; ++d) {
+                    const int64_t k = 2 * n + d;
+                    int64_t b = bond_end_b(L, k);
+                    int satisfied = (int)J[k] * (int)spins[n] * (int)spins[b] > 0;
+                    const uint32_t u = (hi[s] >> (16 * d)) & 0xFFFFu;
+                    int on = 0;
+                    if (satisfied) {
+                        if (thr >= (1ull << 32) || u < thr_hi) {
+                            on = 1;
+                        } else if (u == thr_hi) {
+                            if (!have_lo) {
+                                philox_stream(key, (uint64_t)(32 * c + i), sweep, 3u, lo);
+                                have_lo = 1;
+                            }
+                            const uint32_t v = (lo[s] >> (16 * d)) & 0xFFFFu;
+                            on = ((u << 16) | v) < thr;
+                        }
                     }
-                    const uint32_t v = (lo[h >> 1] >> (16 * (h & 1))) & 0xFFFFu;
-                    on = ((u << 16) | v) < thr;
+                    occ[k] = (uint8_t)on;
                 }
             }
-            occ[k] = (uint8_t)on;
         }
     }
 }

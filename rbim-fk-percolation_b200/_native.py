@@ -107,13 +107,17 @@ def _declare(l):
 
 
 def lib(build_if_missing: bool = True):
-    """The loaded library (built from ``csrc/`` first if it is missing or stale)."""
+    """The loaded library (built from ``csrc/`` first if it is missing or stale).
+
+    ``RBIM_LIBRARY`` in the environment names another build of the same ABI
+    to load instead (a profiling or debug build).
+    """
     global _lib
     with _lock:
         if _lib is not None:
             return _lib
-        path = _build.LIB
-        if build_if_missing:
+        path = os.environ.get("RBIM_LIBRARY") or _build.LIB
+        if build_if_missing and not os.environ.get("RBIM_LIBRARY"):
             try:
                 path = _build.build()
             except Exception as exc:  # pragma: no cover - depends on the toolchain

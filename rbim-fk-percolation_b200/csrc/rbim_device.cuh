@@ -102,17 +102,6 @@ __device__ __forceinline__ uint32_t u4_word(const U4 &v, uint32_t i)
     return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
-// Spread the low 16 bits of v to the even bit positions of a 32-bit word.
-__device__ __forceinline__ uint32_t spread16(uint32_t v)
-{
-    v &= 0xFFFFu;
-    v = (v | (v << 8)) & 0x00FF00FFu;
-    v = (v | (v << 4)) & 0x0F0F0F0Fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
-}
-
 // Mask of bits 0..b inclusive.
 __device__ __forceinline__ uint32_t mask_le(uint32_t b) { return (2u << b) - 1u; }
 
@@ -177,11 +166,11 @@ __device__ __forceinline__ uint32_t xnext_word(const Ld &ld, uint32_t w, const G
     return extract32(ld, s, g);
 }
 
-// Plane word of the +y neighbours (periodic within the row).
+// Plane word of the +y neighbours (periodic within the row); re is the
+// row-end mask of word w (Geom::row_end).
 template <class Ld>
-__device__ __forceinline__ uint32_t ynext_word(const Ld &ld, uint32_t w, const Geom &g)
+__device__ __forceinline__ uint32_t ynext_word(const Ld &ld, uint32_t w, const Geom &g, uint32_t re)
 {
-    const uint32_t re = g.row_end(w);
     uint32_t s1 = (w << 5) + 1u;
     if (s1 >= g.N) s1 -= g.N;
     uint32_t r = extract32(ld, s1, g) & ~re;

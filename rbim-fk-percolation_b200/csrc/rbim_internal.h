@@ -5,7 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/rbim_sm100.h"
+#include "rbim_sm100.h"
 
 namespace rbim {
 
@@ -13,7 +13,8 @@ namespace rbim {
 // sites (n_max <= 65536).
 struct ResidentLayout {
     uint32_t n_max, nw_max, l_max, hs;
-    size_t off_uf, off_S, off_JH, off_JV, off_OH, off_OV, off_FLIP, off_ROOT, off_SEAMV, off_HK, off_HW, bytes;
+    size_t off_uf, off_S, off_JH, off_JV, off_OH, off_OV, off_FLIP, off_ROOT, off_RE, off_SEAMV, off_HK, off_HW,
+        bytes;
 };
 
 ResidentLayout resident_layout(uint32_t l_max, int threads);

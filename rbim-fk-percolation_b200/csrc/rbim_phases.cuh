@@ -29,9 +29,11 @@ struct Lat {
     uint32_t *OH, *OV;     // occupied bonds
     uint32_t *SEAMV;       // occupied y-seam bonds, bit x = row x
     uint32_t *FLIP, *ROOT;
+    const uint32_t *RE;    // row-end masks per word (Geom::row_end), or null to compute them
     int *wrap;             // bit 0 wrap_x, bit 1 wrap_y
     int *err;
     uint32_t cap;
+    __device__ __forceinline__ uint32_t row_end(uint32_t w) const { return RE ? RE[w] : g.row_end(w); }
 };
 
 struct SweepRng {
@@ -53,16 +55,6 @@ __device__ __forceinline__ SweepRng make_rng(uint64_t key, uint64_t sweep, uint6
     return r;
 }
 
-// Spread the low 8 bits of v to bit positions 0, 4, 8, ..., 28.
-__device__ __forceinline__ uint32_t spread8x4(uint32_t v)
-{
-    v &= 0xFFu;
-    v = (v | (v << 12)) & 0x000F000Fu;
-    v = (v | (v << 6)) & 0x03030303u;
-    v = (v | (v << 3)) & 0x11111111u;
-    return v;
-}
-
 // Occupation decision of one bond from its 16-bit draw u: u < thr_hi
 // accepts, u > thr_hi rejects, u == thr_hi (probability 2^-16) defers to the
 // low half v, drawn separately.  Returns 0 reject, 1 accept, 2 undecided.
@@ -75,7 +67,9 @@ __device__ __forceinline__ uint32_t bond_decide(const SweepRng &rng, uint32_t u)
 // (a) Bond activation.  Items are 128-site chunks (four plane words); lane i
 // of the warp owning chunk c draws Philox block 32c + i, whose word s holds
 // the 16-bit draws of the horizontal (low half) and vertical (high half) bond
-// of site 128c + 4i + s.  SEAMV must be zero on entry.
+// of site 128c + 32s + i, i.e. bit i of the chunk's word s, so that each
+// ballot is one word of the occupied-bond planes.  SEAMV must be zero on
+// entry.
 template <class WT>
 __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const SweepRng &rng, uint32_t warp,
                                                      uint32_t nwarps)
@@ -85,25 +79,26 @@ __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const Swe
     const uint32_t nchunks = (g.N + 127u) >> 7;
     Plane S{t.S};
     for (uint32_t c = warp; c < nchunks; c += nwarps) {
-        const uint32_t wl = 4u * c + (lane >> 3);
-        uint32_t sh = 0, sv = 0;
-        if (wl < g.NW) {
-            const uint32_t v = g.valid(wl);
-            const uint32_t s = S(wl);
-            sh = ~(s ^ xnext_word(S, wl, g) ^ t.JH[wl]) & v;
-            sv = ~(s ^ ynext_word(S, wl, g) ^ t.JV[wl]) & v;
+        // Lanes 0..3 form the satisfied masks of the chunk's four words.
+        const uint32_t wq = 4u * c + lane;
+        uint32_t sh = 0, sv = 0, re = 0;
+        if (lane < 4u && wq < g.NW) {
+            re = t.row_end(wq);
+            const uint32_t v = g.valid(wq);
+            const uint32_t s = S(wq);
+            sh = ~(s ^ xnext_word(S, wq, g) ^ t.JH[wq]) & v;
+            sv = ~(s ^ ynext_word(S, wq, g, re) ^ t.JV[wq]) & v;
         }
-        const uint32_t sb = 4u * (lane & 7u);
-        sh = (sh >> sb) & 0xFu;  // satisfied bits of this lane's four sites
-        sv = (sv >> sb) & 0xFu;
         const U4 r = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBond);
         uint32_t dh[4], dv[4];
         bool refine = false;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const uint32_t w = u4_word(r, s);
-            dh[s] = ((sh >> s) & 1u) ? bond_decide(rng, w & 0xFFFFu) : 0u;
-            dv[s] = ((sv >> s) & 1u) ? bond_decide(rng, w >> 16) : 0u;
+            const uint32_t bh = (__shfl_sync(0xFFFFFFFFu, sh, s) >> lane) & 1u;
+            const uint32_t bv = (__shfl_sync(0xFFFFFFFFu, sv, s) >> lane) & 1u;
+            dh[s] = bh ? bond_decide(rng, w & 0xFFFFu) : 0u;
+            dv[s] = bv ? bond_decide(rng, w >> 16) : 0u;
             refine |= (dh[s] == 2u) | (dv[s] == 2u);
         }
         if (refine) {
@@ -120,27 +115,20 @@ __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const Swe
         for (int s = 0; s < 4; ++s) {
             const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
             const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
-            // Word j of the chunk collects lanes 8j .. 8j+7.
-            const uint32_t j = lane & 3u;
-            oh |= spread8x4(bh >> (8u * j)) << s;
-            ov |= spread8x4(bv >> (8u * j)) << s;
+            if (lane == (uint32_t)s) {
+                oh = bh;
+                ov = bv;
+            }
         }
-        if (lane < 8u) {
-            const uint32_t w = 4u * c + (lane & 3u);
-            if (w < g.NW) {
-                if (lane < 4u) {
-                    t.OH[w] = oh;
-                } else {
-                    const uint32_t re = g.row_end(w);
-                    t.OV[w] = ov & ~re;
-                    uint32_t seam = ov & re;
-                    while (seam) {
-                        const uint32_t b = __ffs(seam) - 1u;
-                        seam &= seam - 1u;
-                        const uint32_t x = ((w << 5) + b) / g.L;
-                        atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
-                    }
-                }
+        if (lane < 4u && wq < g.NW) {
+            t.OH[wq] = oh;
+            t.OV[wq] = ov & ~re;
+            uint32_t seam = ov & re;
+            while (seam) {
+                const uint32_t b = __ffs(seam) - 1u;
+                seam &= seam - 1u;
+                const uint32_t x = ((wq << 5) + b) / g.L;
+                atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
             }
         }
     }
@@ -252,37 +240,58 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t warp, uin
     }
 }
 
-// (c) Roots, flip and (optionally) cluster sizes.  Every site is pointed
-// straight at its root (only the site's own thread writes its word here, so
-// after the phase every non-root word holds its root); roots are recorded in
-// ROOT; each site's spin is
-// flipped with its cluster's flip bit; with `count` the root words accumulate
-// the cluster size in their offset field (warp-aggregated with match_any).
-// Returns this warp's number of roots (valid in every lane).
+// (c) Roots of the run heads.  Every parent pointer targets a head (heads
+// are the initial parents, roots are heads, and hooks and path halving only
+// move pointers to roots or grandparents), so once each head points straight
+// at its root, every site reaches its root in two steps.  The walk only
+// reads and each head's thread writes only its own word, so no final pointer
+// can be overwritten by a stale ancestor.  Roots are recorded in ROOT.
+// Returns this warp's number of roots.
 template <class WT>
-__device__ __forceinline__ uint32_t phase_finalize(const Lat<WT> &t, uint32_t warp, uint32_t nwarps, bool flip,
-                                                   bool count)
+__device__ __forceinline__ uint32_t phase_roots(const Lat<WT> &t, uint32_t warp, uint32_t nwarps)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
     uint32_t nroots = 0;
     for (uint32_t w = warp; w < g.NW; w += nwarps) {
         const uint32_t n = (w << 5) + lane;
-        const bool ok = n < g.N;
-        uint32_t r = 0;
-        if (ok) {
+        const bool head = (head_mask(t.OV, w, g.valid(w)) >> lane) & 1u;
+        uint32_t r = n;
+        if (head) {
             r = uf_root_ro<WT>(t.uf, n, t.cap, t.err);
             if (r != n) t.uf.st(n, WT::make(r, 0, 0));
         }
-        const uint32_t roots = __ballot_sync(0xFFFFFFFFu, ok && r == n);
+        const uint32_t roots = __ballot_sync(0xFFFFFFFFu, head && r == n);
+        if (lane == 0) t.ROOT[w] = roots;
+        nroots += __popc(roots);
+    }
+    return nroots;
+}
+
+// (c') Every site: root = parent of parent (after phase_roots), pointed at
+// directly; the spin is flipped with its cluster's flip bit; with `count` the
+// root words accumulate the cluster size in their offset field
+// (warp-aggregated with match_any).
+template <class WT>
+__device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uint32_t nwarps, bool flip, bool count)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const Geom &g = t.g;
+    for (uint32_t w = warp; w < g.NW; w += nwarps) {
+        const uint32_t n = (w << 5) + lane;
+        const bool ok = n < g.N;
+        uint32_t r = 0;
+        if (ok) {
+            const uint32_t p = WT::parent(t.uf.ld(n));
+            r = WT::parent(t.uf.ld(p));
+            if (r != p) t.uf.st(n, WT::make(r, 0, 0));
+        }
         if (flip) {
             const uint32_t fl = ok ? (t.FLIP[r >> 5] >> (r & 31u)) & 1u : 0u;
             const uint32_t s = t.S[w];
             const uint32_t ns = __ballot_sync(0xFFFFFFFFu, ok && (((s >> lane) & 1u) ^ fl)) & g.valid(w);
             if (lane == 0) t.S[w] = ns;
         }
-        if (lane == 0) t.ROOT[w] = roots;
-        nroots += __popc(roots);
         if (count) {
             const uint32_t live = __ballot_sync(0xFFFFFFFFu, ok);
             if (ok) {
@@ -291,20 +300,20 @@ __device__ __forceinline__ uint32_t phase_finalize(const Lat<WT> &t, uint32_t wa
             }
         }
     }
-    return nroots;
 }
 
 // (d) Unsatisfied bonds and down spins over words first, first+stride, ...
-__device__ __forceinline__ void measure_energy(const Geom &g, const uint32_t *S, const uint32_t *JH,
-                                               const uint32_t *JV, uint32_t first, uint32_t stride,
-                                               uint32_t &unsat, uint32_t &downs)
+template <class WT>
+__device__ __forceinline__ void measure_energy(const Lat<WT> &t, uint32_t first, uint32_t stride, uint32_t &unsat,
+                                               uint32_t &downs)
 {
-    Plane Sp{const_cast<uint32_t *>(S)};
+    const Geom &g = t.g;
+    Plane Sp{t.S};
     for (uint32_t w = first; w < g.NW; w += stride) {
         const uint32_t v = g.valid(w);
         const uint32_t s = Sp(w);
-        unsat += __popc((s ^ xnext_word(Sp, w, g) ^ JH[w]) & v);
-        unsat += __popc((s ^ ynext_word(Sp, w, g) ^ JV[w]) & v);
+        unsat += __popc((s ^ xnext_word(Sp, w, g) ^ t.JH[w]) & v);
+        unsat += __popc((s ^ ynext_word(Sp, w, g, t.row_end(w)) ^ t.JV[w]) & v);
         downs += __popc(s & v);
     }
 }

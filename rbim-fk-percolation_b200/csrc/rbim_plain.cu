@@ -127,6 +127,7 @@ __device__ __forceinline__ Lat<Word64> plain_lat(const PlainArgs &a)
     t.FLIP = a.ws.FLIP;
     t.ROOT = a.ws.ROOT;
     t.SEAMV = a.ws.SEAMV;
+    t.RE = nullptr;
     t.wrap = &a.ws.sc->wrap;
     t.err = &a.ws.sc->err;
     t.cap = t.g.N + 64u;
@@ -168,13 +169,20 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_union(PlainArgs a)
     phase_union<Word64>(plain_lat(a), gwarp(), gnwarps(), gtid(), gnthreads());
 }
 
+__global__ void __launch_bounds__(kPlainThreads) k_plain_roots(PlainArgs a)
+{
+    if (!chain_phase(a.chain)) return;
+    const Lat<Word64> t = plain_lat(a);
+    const uint32_t nr = phase_roots<Word64>(t, gwarp(), gnwarps());
+    if ((threadIdx.x & 31u) == 0 && nr) atomicAdd(&a.ws.sc->nroots, nr);
+}
+
 __global__ void __launch_bounds__(kPlainThreads) k_plain_finalize(PlainArgs a)
 {
     const int ph = chain_phase(a.chain);
     if (!ph) return;
     const Lat<Word64> t = plain_lat(a);
-    const uint32_t nr = phase_finalize<Word64>(t, gwarp(), gnwarps(), true, ph == 2);
-    if ((threadIdx.x & 31u) == 0 && nr) atomicAdd(&a.ws.sc->nroots, nr);
+    phase_sites<Word64>(t, gwarp(), gnwarps(), true, ph == 2);
     for (uint32_t i = gtid(); i < (t.g.L + 31u) / 32u; i += gnthreads()) t.SEAMV[i] = 0u;
 }
 
@@ -183,7 +191,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
     if (chain_phase(a.chain) != 2) return;
     const Lat<Word64> t = plain_lat(a);
     uint32_t unsat = 0, downs = 0;
-    measure_energy(t.g, t.S, t.JH, t.JV, gtid(), gnthreads(), unsat, downs);
+    measure_energy(t, gtid(), gnthreads(), unsat, downs);
     unsigned long long k1 = 0, k2 = 0;
     for (uint32_t w = gtid(); w < t.g.NW; w += gnthreads()) {
         uint32_t roots = t.ROOT[w];
@@ -347,6 +355,7 @@ __device__ __forceinline__ Lat<Word64> label_lat(const PlainWs &ws, uint32_t L)
     t.FLIP = ws.FLIP;
     t.ROOT = ws.ROOT;
     t.SEAMV = ws.SEAMV;
+    t.RE = nullptr;
     t.wrap = &ws.sc->wrap;
     t.err = &ws.sc->err;
     t.cap = t.g.N + 64u;
@@ -363,9 +372,14 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_label_union(PlainWs ws,
     phase_union<Word64>(label_lat(ws, L), gwarp(), gnwarps(), gtid(), gnthreads());
 }
 
+__global__ void __launch_bounds__(kPlainThreads) k_plain_label_roots(PlainWs ws, uint32_t L)
+{
+    phase_roots<Word64>(label_lat(ws, L), gwarp(), gnwarps());
+}
+
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_finalize(PlainWs ws, uint32_t L)
 {
-    phase_finalize<Word64>(label_lat(ws, L), gwarp(), gnwarps(), false, false);
+    phase_sites<Word64>(label_lat(ws, L), gwarp(), gnwarps(), false, false);
 }
 
 // Exclusive prefix of root counts per word (single CTA) into the FLIP plane.
@@ -434,6 +448,7 @@ cudaError_t launch_plain_sweeps(rbim_chain_t *chain, uint32_t *spin_pool, const 
         k_plain_activate<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_heads<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_union<<<grid, kPlainThreads, 0, stream>>>(a);
+        k_plain_roots<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_finalize<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_measure1<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_measure2<<<1, 1024, 0, stream>>>(a, grid);
@@ -453,6 +468,7 @@ cudaError_t launch_plain_label(int64_t L, const uint8_t *occ, int32_t *labels, i
     k_plain_label_load<<<grid, kPlainThreads, 0, stream>>>(ws, l, occ);
     k_plain_label_heads<<<grid, kPlainThreads, 0, stream>>>(ws, l);
     k_plain_label_union<<<grid, kPlainThreads, 0, stream>>>(ws, l);
+    k_plain_label_roots<<<grid, kPlainThreads, 0, stream>>>(ws, l);
     k_plain_label_finalize<<<grid, kPlainThreads, 0, stream>>>(ws, l);
     k_plain_label_scan<<<1, 1024, 0, stream>>>(ws, l);
     k_plain_label_write<<<grid, kPlainThreads, 0, stream>>>(ws, l, labels, n_clusters, wraps, status);

@@ -46,6 +46,30 @@ uint32_t hash_size(uint32_t l_max)
 
 }  // namespace
 
+// Optional per-phase cycle accounting (profiling builds only, compiled with
+// -DRBIM_PROFILE_PHASES): thread 0 adds the cycles since the previous mark to
+// a per-phase counter at each barrier.  No work is skipped.
+#ifdef RBIM_PROFILE_PHASES
+__device__ unsigned long long g_phase_cycles[16];
+__device__ __forceinline__ void phase_mark(int k)
+{
+    __shared__ long long s_t;
+    if (threadIdx.x == 0) {
+        const long long now = clock64();
+        if (k >= 0) atomicAdd(&g_phase_cycles[k], (unsigned long long)(now - s_t));
+        s_t = now;
+    }
+}
+#define RBIM_PHASE_MARK(k) phase_mark(k)
+__device__ unsigned long long g_event_counts[8];
+#define RBIM_COUNT(k, v) atomicAdd(&g_event_counts[k], (unsigned long long)(v))
+#define RBIM_PROF_ONLY(...) __VA_ARGS__
+#else
+#define RBIM_PHASE_MARK(k) ((void)0)
+#define RBIM_COUNT(k, v) ((void)0)
+#define RBIM_PROF_ONLY(...)
+#endif
+
 // Open-lattice union-find word: the parent site only.
 struct Word16 {
     using T = unsigned short;
@@ -54,6 +78,35 @@ struct Word16 {
     __device__ __forceinline__ static int oy(T) { return 0; }
     __device__ __forceinline__ static T make(uint32_t p, int, int) { return (T)p; }
     __device__ __forceinline__ static T count_inc(uint32_t c) { return (T)c; }
+};
+
+// The open union-find lives in shared memory: access it through 32-bit
+// shared-window addresses with explicit ld/st/atom.shared instructions.
+template <>
+struct UF<Word16> {
+    using T = unsigned short;
+    T *w;          // generic pointer (for code that indexes the array directly)
+    uint32_t sa;   // shared-window address of w
+    __device__ __forceinline__ T ld(uint32_t i) const
+    {
+        T v;
+        asm volatile("ld.volatile.shared.u16 %0, [%1];" : "=h"(v) : "r"(sa + 2u * i) : "memory");
+        return v;
+    }
+    __device__ __forceinline__ void st(uint32_t i, T v) const
+    {
+        asm volatile("st.volatile.shared.u16 [%0], %1;" ::"r"(sa + 2u * i), "h"(v) : "memory");
+    }
+    __device__ __forceinline__ T cas(uint32_t i, T expect, T v) const
+    {
+        T old;
+        asm volatile("atom.shared.cas.b16 %0, [%1], %2, %3;"
+                     : "=h"(old)
+                     : "r"(sa + 2u * i), "h"(expect), "h"(v)
+                     : "memory");
+        return old;
+    }
+    __device__ __forceinline__ void add(uint32_t i, T v) const { uf_atomic_add(w + i, v); }
 };
 
 // Seam union-find word: parent slot (12 bits) | wx (10 bits) | wy (10 bits),
@@ -96,6 +149,8 @@ ResidentLayout resident_layout(uint32_t l_max, int threads)
     ly.off_FLIP = off;
     off += plane;
     ly.off_ROOT = off;
+    off += plane;
+    ly.off_RE = off;
     off += plane;
     ly.off_SEAMV = off;
     off = align16(off + 4ull * (((l_max + 31u) / 32u) + 4u));
@@ -162,6 +217,7 @@ __device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayou
     Lat<Word16> &t = r.t;
     t.g = Geom{L, L * L, (L * L + 31u) / 32u};
     t.uf.w = (unsigned short *)(smem + ly.off_uf);
+    t.uf.sa = (uint32_t)__cvta_generic_to_shared(t.uf.w);
     t.S = (uint32_t *)(smem + ly.off_S);
     t.JH = (const uint32_t *)(smem + ly.off_JH);
     t.JV = (const uint32_t *)(smem + ly.off_JV);
@@ -169,6 +225,7 @@ __device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayou
     t.OV = (uint32_t *)(smem + ly.off_OV);
     t.FLIP = (uint32_t *)(smem + ly.off_FLIP);
     t.ROOT = (uint32_t *)(smem + ly.off_ROOT);
+    t.RE = (const uint32_t *)(smem + ly.off_RE);
     t.SEAMV = (uint32_t *)(smem + ly.off_SEAMV);
     t.wrap = &red.wrap;
     t.err = &red.err;
@@ -178,6 +235,14 @@ __device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayou
     r.hs = ly.hs;
     r.hs_log2 = 31u - __clz(ly.hs);
     return r;
+}
+
+// Row-end masks of the lattice (computed once per chain, so that the sweep
+// needs no integer division).
+__device__ __forceinline__ void init_row_ends(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
+{
+    uint32_t *re = const_cast<uint32_t *>(t.RE);
+    for (uint32_t w = tid; w < t.g.NW; w += nthreads) re[w] = t.g.row_end(w);
 }
 
 // Mask of the bits of word w whose site lies in the last row (x = L-1): the
@@ -191,44 +256,130 @@ __device__ __forceinline__ uint32_t last_row_mask(const Geom &g, uint32_t w)
     return ~((1u << (first - n0)) - 1u) & v;
 }
 
-// Open-lattice union: hook the larger root under the smaller with a 16-bit CAS.
-__device__ __forceinline__ void union_open(const UF<Word16> &uf, uint32_t a, uint32_t b, uint32_t cap, int *err)
-{
-    for (uint32_t it = 0; it < cap; ++it) {
-        a = uf_root<Word16>(uf, a, cap, err);
-        b = uf_root<Word16>(uf, b, cap, err);
-        if (a == b) return;
-        if (a > b) {
-            const uint32_t x = a;
-            a = b;
-            b = x;
-        }
-        if (uf.cas(b, (unsigned short)b, (unsigned short)a) == (unsigned short)b) return;
+// Root of x in the open union-find, with path halving; adds the number of
+// Work slices.  Pointer chasing has data-dependent length, so the union and
+// root phases run as flat per-thread loops that take one pointer step per
+// iteration and fetch the next item as soon as the current one is done; a
+// thread's cost is then the sum of its items' steps rather than a per-round
+// maximum over the warp.  Thread t owns the bit ranges t, t + T, t + 2T, ...
+// where each word is cut into `seg` equal ranges (seg is a power of two
+// chosen so that small lattices still give every thread work).
+struct Slices {
+    uint32_t seg_log2, bits, items;
+    __device__ __forceinline__ uint32_t word(uint32_t i) const { return i >> seg_log2; }
+    __device__ __forceinline__ uint32_t mask(uint32_t i) const
+    {
+        const uint32_t s = i & ((1u << seg_log2) - 1u);
+        return (bits == 32u ? 0xFFFFFFFFu : ((1u << bits) - 1u)) << (s * bits);
     }
-    atomicOr(err, kErrUnionCap);
+};
+
+__device__ __forceinline__ Slices make_slices(uint32_t NW, uint32_t nthreads)
+{
+    uint32_t lg = 0;
+    while (lg < 5u && (NW << (lg + 1u)) <= nthreads) ++lg;
+    return Slices{lg, 32u >> lg, NW << lg};
+}
+
+// Occupied x-bonds of word w that need a union: off the x seam, and not
+// already connected through an elementary plaquette with the bond before.
+__device__ __forceinline__ uint32_t union_need(const Lat<Word16> &t, uint32_t w)
+{
+    const Geom &g = t.g;
+    const uint32_t oh = t.OH[w] & ~last_row_mask(g, w);
+    if (!oh) return 0u;
+    Plane OVp{t.OV};
+    const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
+    const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
+    const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
+    const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
+    uint32_t s = (w << 5) + g.L - 1u;
+    if (s >= g.N) s -= g.N;
+    return oh & ~(prev_oh & prev_ov & extract32(OVp, s, g));
+}
+
+// One path-halving step of a walk at x, without branches: returns the next
+// position and sets `done` when x's parent or grandparent is the root (the
+// returned position is then the root).
+__device__ __forceinline__ uint32_t halving_step(const UF<Word16> &uf, uint32_t x, bool &done)
+{
+    const uint32_t p = uf.ld(x);
+    const uint32_t gp = uf.ld(p);
+    const bool x_root = p == x, p_root = gp == p;
+    if (!x_root && !p_root) uf.st(x, (unsigned short)gp);
+    done = x_root || p_root;
+    return x_root ? x : (p_root ? p : gp);
 }
 
 // (b) Open-lattice unions across occupied x-bonds that do not cross the x
-// seam; the plaquette rule of phase_union skips bonds already connected.
-__device__ __forceinline__ void phase_union_open(const Lat<Word16> &t, uint32_t warp, uint32_t nwarps)
+// seam: the larger root is hooked under the smaller with a 16-bit CAS, finds
+// use path halving, and a union whose CAS loses a race restarts from the two
+// roots it found.  Both endpoint walks advance in the same loop iteration.
+__device__ __forceinline__ void phase_union_open(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
 {
-    const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
-    Plane OVp{t.OV};
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t oh = t.OH[w] & ~last_row_mask(g, w);
-        if (!oh) continue;
-        const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
-        const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
-        const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
-        const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
-        const uint32_t prev_ovx = extract32(OVp, ((w << 5) + g.L - 1u) % g.N, g);
-        const uint32_t need = oh & ~(prev_oh & prev_ov & prev_ovx);
-        if ((need >> lane) & 1u) {
-            const uint32_t n = (w << 5) + lane;
-            union_open(t.uf, n, n + g.L, t.cap, t.err);
+    const UF<Word16> &uf = t.uf;
+    const Slices sl = make_slices(g.NW, nthreads);
+    uint32_t item = tid, pending = 0, base = 0;
+    uint32_t xa = 0, xb = 0;
+    bool fetch = true;
+    const uint32_t cap = 64u * g.N + 4096u;
+    uint32_t it = 0;
+    RBIM_PROF_ONLY(uint32_t n_bonds = 0; uint32_t n_fails = 0);
+    for (;; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrUnionCap);
+            break;
+        }
+        if (fetch) {
+            while (!pending && item < sl.items) {
+                const uint32_t w = sl.word(item);
+                pending = union_need(t, w) & sl.mask(item);
+                base = w << 5;
+                item += nthreads;
+            }
+            if (!pending) break;
+            xa = base + (uint32_t)(__ffs(pending) - 1);
+            pending &= pending - 1u;
+            xb = xa + g.L;
+            fetch = false;
+            RBIM_PROF_ONLY(++n_bonds);
+        }
+        bool da, db;
+        xa = halving_step(uf, xa, da);
+        xb = halving_step(uf, xb, db);
+        if (da && db) {
+            // Both walks are at roots.
+            if (xa == xb) {
+                fetch = true;
+            } else {
+                const uint32_t lo = min(xa, xb), hi = max(xa, xb);
+                fetch = uf.cas(hi, (unsigned short)hi, (unsigned short)lo) == (unsigned short)hi;
+                // A lost race leaves both walks at their old roots, to resume from.
+                RBIM_PROF_ONLY(n_fails += fetch ? 0u : 1u);
+            }
         }
     }
+#ifdef RBIM_PROFILE_PHASES
+    {
+        uint32_t mx = it, sm = it;
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+            sm += __shfl_xor_sync(0xFFFFFFFFu, sm, o);
+        }
+        uint32_t nb = n_bonds, nf = n_fails;
+        for (int o = 16; o > 0; o >>= 1) {
+            nb += __shfl_xor_sync(0xFFFFFFFFu, nb, o);
+            nf += __shfl_xor_sync(0xFFFFFFFFu, nf, o);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            RBIM_COUNT(3, mx);
+            RBIM_COUNT(4, sm);
+            RBIM_COUNT(0, nb);
+            RBIM_COUNT(2, nf);
+        }
+    }
+#endif
 }
 
 __device__ __forceinline__ uint32_t hash_insert(const Res &r, uint32_t key, int *err)
@@ -325,6 +476,78 @@ __device__ __forceinline__ void phase_seam_propagate(const Res &r, uint32_t tid,
     }
 }
 
+// (c) Roots of the run heads (see phase_roots), as a flat per-thread loop
+// over the heads of the thread's slices: read-only walks, each head's final
+// root written by the head's own thread.  ROOT must be zero on entry.
+// Returns the number of roots this thread found.
+// Next head of the thread's slices into (h, x), or false when there is none.
+__device__ __forceinline__ bool next_head(const Lat<Word16> &t, const Slices &sl, uint32_t nthreads, uint32_t &item,
+                                          uint32_t &pending, uint32_t &base, uint32_t &h)
+{
+    while (!pending && item < sl.items) {
+        const uint32_t w = sl.word(item);
+        pending = head_mask(t.OV, w, t.g.valid(w)) & sl.mask(item);
+        base = w << 5;
+        item += nthreads;
+    }
+    if (!pending) return false;
+    h = base + (uint32_t)(__ffs(pending) - 1);
+    pending &= pending - 1u;
+    return true;
+}
+
+__device__ __forceinline__ uint32_t phase_roots_flat(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
+{
+    const Geom &g = t.g;
+    const Slices sl = make_slices(g.NW, nthreads);
+    uint32_t item = tid, pending = 0, base = 0, nroots = 0;
+    // Two walks in flight per thread: heads h0, h1 at positions x0, x1.
+    uint32_t h0 = 0, h1 = 0, x0 = 0, x1 = 0;
+    bool a0 = next_head(t, sl, nthreads, item, pending, base, h0);
+    bool a1 = a0 && next_head(t, sl, nthreads, item, pending, base, h1);
+    x0 = h0;
+    x1 = h1;
+    const uint32_t cap = 64u * g.N + 4096u;
+    for (uint32_t it = 0; a0 || a1; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrFindCap);
+            break;
+        }
+        const uint32_t p0 = t.uf.ld(x0), p1 = t.uf.ld(x1);
+        const bool r0 = a0 && p0 == x0, r1 = a1 && p1 == x1;
+        x0 = p0;
+        x1 = p1;
+        if (r0) {
+            if (x0 != h0) {
+                t.uf.st(h0, (unsigned short)x0);
+            } else {
+                atomicOr(t.ROOT + (h0 >> 5), 1u << (h0 & 31u));
+                ++nroots;
+            }
+            a0 = next_head(t, sl, nthreads, item, pending, base, h0);
+            x0 = h0;
+        }
+        if (r1) {
+            if (x1 != h1) {
+                t.uf.st(h1, (unsigned short)x1);
+            } else {
+                atomicOr(t.ROOT + (h1 >> 5), 1u << (h1 & 31u));
+                ++nroots;
+            }
+            a1 = next_head(t, sl, nthreads, item, pending, base, h1);
+            x1 = h1;
+        }
+    }
+    return nroots;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
 // The labelling stages shared by the sweep and label kernels, from occupied
 // bond planes to final roots; barriers between stages.  Returns the number of
 // roots counted by this warp.
@@ -335,16 +558,25 @@ __device__ __forceinline__ uint32_t resident_label(const Res &r, bool flip)
     constexpr uint32_t nwarps = NT / 32;
     phase_heads<Word16>(r.t, warp, nwarps);
     seam_reset(r, tid, NT);
+    for (uint32_t w = tid; w < r.t.g.NW; w += NT) r.t.ROOT[w] = 0u;
     __syncthreads();
-    phase_union_open(r.t, warp, nwarps);
+    RBIM_PHASE_MARK(1);
+    phase_union_open(r.t, tid, NT);
     __syncthreads();
+    RBIM_PHASE_MARK(2);
     phase_seam(r, tid, NT);
     __syncthreads();
+    RBIM_PHASE_MARK(3);
     phase_seam_propagate(r, tid, NT);
     for (uint32_t i = tid; i < (r.t.g.L + 31u) / 32u; i += NT) r.t.SEAMV[i] = 0u;
     __syncthreads();
-    const uint32_t nr = phase_finalize<Word16>(r.t, warp, nwarps, flip, false);
+    RBIM_PHASE_MARK(4);
+    const uint32_t nr = warp_sum(phase_roots_flat(r.t, tid, NT));
     __syncthreads();
+    RBIM_PHASE_MARK(11);
+    phase_sites<Word16>(r.t, warp, nwarps, flip, false);
+    __syncthreads();
+    RBIM_PHASE_MARK(5);
     return nr;
 }
 
@@ -371,7 +603,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
 
     // Energy and magnetization of the flipped spins; root counters to zero.
     uint32_t unsat = 0, downs = 0;
-    measure_energy(g, t.S, t.JH, t.JV, tid, NT, unsat, downs);
+    measure_energy(t, tid, NT, unsat, downs);
     for (uint32_t w = tid; w < g.NW; w += NT) {
         uint32_t roots = t.ROOT[w];
         while (roots) {
@@ -391,6 +623,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         red.roots[warp] = nroots_warp;
     }
     __syncthreads();
+    RBIM_PHASE_MARK(6);
     if (warp == 0) {
         uint32_t u = lane < nwarps ? red.unsat[lane] : 0u, d = lane < nwarps ? red.downs[lane] : 0u;
         uint32_t nr = lane < nwarps ? red.roots[lane] : 0u;
@@ -406,19 +639,21 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             red.downs_t = d;
         }
     }
-    // Cluster sizes into the root words (warp-aggregated per root).
+    // Cluster sizes into the root words: one add per piece of run inside a
+    // word (a run shares its root), made by the piece's first site.
     for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t n = (w << 5) + lane;
-        const bool ok = n < g.N;
-        uint32_t r = 0;
-        if (ok) r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
-        const uint32_t live = __ballot_sync(0xFFFFFFFFu, ok);
-        if (ok) {
-            const uint32_t grp = __match_any_sync(live, r);
-            if (lane == (uint32_t)(__ffs(grp) - 1)) add16(u16, r, __popc(grp));
+        const uint32_t valid = g.valid(w);
+        const uint32_t lead = (head_mask(t.OV, w, valid) | 1u) & valid;
+        if ((lead >> lane) & 1u) {
+            const uint32_t n = (w << 5) + lane;
+            const uint32_t next = lead & ~mask_le(lane);
+            const uint32_t end = next ? (uint32_t)(__ffs(next) - 1) : (uint32_t)__popc(valid);
+            const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
+            add16(u16, r, end - lane);
         }
     }
     __syncthreads();
+    RBIM_PHASE_MARK(7);
     const uint32_t ncl = red.ncl;
     if (ncl > 1) {
         uint32_t k1 = 0, k2 = 0;
@@ -447,6 +682,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             }
         }
         __syncthreads();
+        RBIM_PHASE_MARK(8);
         const uint32_t g1 = red.g1;
         int mc = 0;
         for (uint32_t w = warp; w < g.NW; w += nwarps) {
@@ -458,6 +694,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         }
         if (lane == 0) red.mc[warp] = mc;
         __syncthreads();
+        RBIM_PHASE_MARK(9);
     } else if (tid == 0) {
         // One cluster covers the lattice.
         red.g1 = 0;
@@ -529,6 +766,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
                 ((uint4 *)t.JV)[i] = gv[i];
             }
             for (uint32_t i = tid; i < (L + 31u) / 32u; i += NT) t.SEAMV[i] = 0u;
+            init_row_ends(t, tid, NT);
         }
         const uint64_t t_end = (uint64_t)ch.n_therm + (uint64_t)ch.n_bins * (uint64_t)ch.sweeps_per_bin;
         uint64_t sweep = ch.sweep;
@@ -538,8 +776,10 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
         for (; sweep < stop; ++sweep) {
             const bool measure = sweep >= (uint64_t)ch.n_therm;
             if (tid == 0) red.wrap = 0;
+            RBIM_PHASE_MARK(-1);
             phase_activate<Word16>(t, make_rng(ch.key, sweep, ch.thr), warp, nwarps, tid, NT);
             __syncthreads();
+            RBIM_PHASE_MARK(0);
             const uint32_t nr = resident_label<NT>(res, true);
             if (measure) {
                 long long rec[kRecLen];
@@ -563,6 +803,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
                         for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];
                     }
                 }
+                RBIM_PHASE_MARK(10);
             }
         }
         if (tid == 0) {
@@ -601,6 +842,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
     const Geom g = t.g;
     const uint8_t *o = occ + lat * 2ull * g.N;
     for (uint32_t i = tid; i < (L + 31u) / 32u; i += NT) t.SEAMV[i] = 0u;
+    init_row_ends(t, tid, NT);
     __syncthreads();
     for (uint32_t w = tid; w < g.NW; w += NT) {
         uint32_t h = 0, v = 0;
@@ -740,3 +982,28 @@ cudaError_t launch_resident_label(int L, int n_lattices, const uint8_t *occ, int
 }
 
 }  // namespace rbim
+
+#ifdef RBIM_PROFILE_PHASES
+// Profiling builds only: copy out (and optionally reset) the per-phase cycle
+// counters of the resident engine.
+extern "C" int rbim_profile_phase_cycles(unsigned long long *out, int reset)
+{
+    cudaError_t e = cudaMemcpyFromSymbol(out, rbim::g_phase_cycles, sizeof(unsigned long long) * 16);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long z[16] = {};
+        e = cudaMemcpyToSymbol(rbim::g_phase_cycles, z, sizeof(z));
+    }
+    return e == cudaSuccess ? 0 : -2;
+}
+
+// Profiling builds only: event counters (0 unions, 1 find steps, 2 failed CAS).
+extern "C" int rbim_profile_event_counts(unsigned long long *out, int reset)
+{
+    cudaError_t e = cudaMemcpyFromSymbol(out, rbim::g_event_counts, sizeof(unsigned long long) * 8);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long z[8] = {};
+        e = cudaMemcpyToSymbol(rbim::g_event_counts, z, sizeof(z));
+    }
+    return e == cudaSuccess ? 0 : -2;
+}
+#endif
