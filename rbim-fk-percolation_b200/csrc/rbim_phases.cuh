@@ -78,57 +78,69 @@ __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const Swe
     const Geom &g = t.g;
     const uint32_t nchunks = (g.N + 127u) >> 7;
     Plane S{t.S};
-    for (uint32_t c = warp; c < nchunks; c += nwarps) {
-        // Lanes 0..3 form the satisfied masks of the chunk's four words.
-        const uint32_t wq = 4u * c + lane;
-        uint32_t sh = 0, sv = 0, re = 0;
-        if (lane < 4u && wq < g.NW) {
-            re = t.row_end(wq);
-            const uint32_t v = g.valid(wq);
-            const uint32_t s = S(wq);
-            sh = ~(s ^ xnext_word(S, wq, g) ^ t.JH[wq]) & v;
-            sv = ~(s ^ ynext_word(S, wq, g, re) ^ t.JV[wq]) & v;
-        }
-        const U4 r = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBond);
-        uint32_t dh[4], dv[4];
-        bool refine = false;
+    // Two chunks per iteration (c and c + nwarps): two independent Philox
+    // evaluations per lane.
+    for (uint32_t c0 = warp; c0 < nchunks; c0 += 2u * nwarps) {
+        uint32_t sh[2], sv[2], re[2], wq[2];
+        U4 r[2];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const uint32_t w = u4_word(r, s);
-            const uint32_t bh = (__shfl_sync(0xFFFFFFFFu, sh, s) >> lane) & 1u;
-            const uint32_t bv = (__shfl_sync(0xFFFFFFFFu, sv, s) >> lane) & 1u;
-            dh[s] = bh ? bond_decide(rng, w & 0xFFFFu) : 0u;
-            dv[s] = bv ? bond_decide(rng, w >> 16) : 0u;
-            refine |= (dh[s] == 2u) | (dv[s] == 2u);
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t c = c0 + k * nwarps;
+            // Lanes 0..3 form the satisfied masks of the chunk's four words.
+            wq[k] = 4u * c + lane;
+            sh[k] = sv[k] = re[k] = 0;
+            if (lane < 4u && wq[k] < g.NW) {
+                re[k] = t.row_end(wq[k]);
+                const uint32_t v = g.valid(wq[k]);
+                const uint32_t s = S(wq[k]);
+                sh[k] = ~(s ^ xnext_word(S, wq[k], g) ^ t.JH[wq[k]]) & v;
+                sv[k] = ~(s ^ ynext_word(S, wq[k], g, re[k]) ^ t.JV[wq[k]]) & v;
+            }
+            r[k] = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBond);
         }
-        if (refine) {
-            const U4 q = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBondLow);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t c = c0 + k * nwarps;
+            uint32_t dh[4], dv[4];
+            bool refine = false;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const uint32_t w = u4_word(q, s);
-                if (dh[s] == 2u) dh[s] = (w & 0xFFFFu) < rng.thr_lo ? 1u : 0u;
-                if (dv[s] == 2u) dv[s] = (w >> 16) < rng.thr_lo ? 1u : 0u;
+                const uint32_t w = u4_word(r[k], s);
+                const uint32_t bh = (__shfl_sync(0xFFFFFFFFu, sh[k], s) >> lane) & 1u;
+                const uint32_t bv = (__shfl_sync(0xFFFFFFFFu, sv[k], s) >> lane) & 1u;
+                dh[s] = bh ? bond_decide(rng, w & 0xFFFFu) : 0u;
+                dv[s] = bv ? bond_decide(rng, w >> 16) : 0u;
+                refine |= (dh[s] == 2u) | (dv[s] == 2u);
             }
-        }
-        uint32_t oh = 0, ov = 0;
+            if (refine) {
+                const U4 q = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBondLow);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
-            const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
-            if (lane == (uint32_t)s) {
-                oh = bh;
-                ov = bv;
+                for (int s = 0; s < 4; ++s) {
+                    const uint32_t w = u4_word(q, s);
+                    if (dh[s] == 2u) dh[s] = (w & 0xFFFFu) < rng.thr_lo ? 1u : 0u;
+                    if (dv[s] == 2u) dv[s] = (w >> 16) < rng.thr_lo ? 1u : 0u;
+                }
             }
-        }
-        if (lane < 4u && wq < g.NW) {
-            t.OH[wq] = oh;
-            t.OV[wq] = ov & ~re;
-            uint32_t seam = ov & re;
-            while (seam) {
-                const uint32_t b = __ffs(seam) - 1u;
-                seam &= seam - 1u;
-                const uint32_t x = ((wq << 5) + b) / g.L;
-                atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
+            uint32_t oh = 0, ov = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
+                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
+                if (lane == (uint32_t)s) {
+                    oh = bh;
+                    ov = bv;
+                }
+            }
+            if (lane < 4u && wq[k] < g.NW) {
+                t.OH[wq[k]] = oh;
+                t.OV[wq[k]] = ov & ~re[k];
+                uint32_t seam = ov & re[k];
+                while (seam) {
+                    const uint32_t b = __ffs(seam) - 1u;
+                    seam &= seam - 1u;
+                    const uint32_t x = ((wq[k] << 5) + b) / g.L;
+                    atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
+                }
             }
         }
     }
@@ -164,36 +176,59 @@ __device__ __forceinline__ void phase_activate(const Lat<WT> &t, const SweepRng 
 // always heads).
 __device__ __forceinline__ uint32_t head_mask(const uint32_t *OV, uint32_t w, uint32_t valid)
 {
-    const uint32_t ov = *((volatile const uint32_t *)(OV + w));
-    const uint32_t prev = w ? (*((volatile const uint32_t *)(OV + w - 1u)) >> 31) : 0u;
+    const uint32_t ov = OV[w];
+    const uint32_t prev = w ? (OV[w - 1u] >> 31) : 0u;
     return ~((ov << 1) | prev) & valid;
 }
 
 // (b) Union-find initialisation: every site points at the head of its run of
-// occupied y-bonds with zero image offset (runs never cross a seam).
+// occupied y-bonds with zero image offset (runs never cross a seam).  A warp
+// takes B consecutive words at a time: lane j finds the last head of word j,
+// a max-scan over the lanes gives every word the last head before it, and
+// the warp then writes the B words one after the other, one site per lane.
 template <class WT>
 __device__ __forceinline__ void phase_heads(const Lat<WT> &t, uint32_t warp, uint32_t nwarps)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t h = head_mask(t.OV, w, g.valid(w));
-        uint32_t carry = 0;
-        if (!(h & 1u)) {
-            // Last head in an earlier word (site 0 is always a head).
-            for (uint32_t ww = w; ww-- > 0;) {
+    uint32_t B = 32;
+    while (B > 1u && B * nwarps > g.NW) B >>= 1;
+    for (uint32_t base = warp * B; base < g.NW; base += nwarps * B) {
+        const uint32_t wj = base + lane;
+        const bool has = lane < B && wj < g.NW;
+        const uint32_t h = has ? head_mask(t.OV, wj, g.valid(wj)) : 0u;
+        // Positions are stored + 1, so that 0 means "no head yet".
+        uint32_t pre = 0;  // last head before word base (lane 0)
+        if (lane == 0 && base > 0 && !(h & 1u)) {
+            // Site 0 always heads a run, so this walk back ends.
+            for (uint32_t ww = base; ww-- > 0;) {
                 const uint32_t hh = head_mask(t.OV, ww, 0xFFFFFFFFu);
                 if (hh) {
-                    carry = (ww << 5) + 31u - __clz(hh);
+                    pre = (ww << 5) + 32u - __clz(hh);
                     break;
                 }
             }
         }
-        const uint32_t n = (w << 5) + lane;
-        if (n < g.N) {
-            const uint32_t m = h & mask_le(lane);
-            const uint32_t head = m ? (w << 5) + 31u - __clz(m) : carry;
-            t.uf.st(n, WT::make(head, 0, 0));
+        uint32_t incl = max(h ? (wj << 5) + 32u - __clz(h) : 0u, pre);
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl = max(incl, v);
+        }
+        // Last head before word j: the scan of lanes < j, or pre for j = 0.
+        uint32_t before = __shfl_up_sync(0xFFFFFFFFu, incl, 1);
+        if (lane == 0) before = pre;
+        for (uint32_t j = 0; j < B; ++j) {
+            const uint32_t w = base + j;
+            if (w >= g.NW) break;
+            const uint32_t hj = __shfl_sync(0xFFFFFFFFu, h, j);
+            const uint32_t cj = __shfl_sync(0xFFFFFFFFu, before, j);
+            const uint32_t n = (w << 5) + lane;
+            if (n < g.N) {
+                const uint32_t m = hj & mask_le(lane);
+                const uint32_t head = m ? (w << 5) + 31u - __clz(m) : cj - 1u;
+                t.uf.st(n, WT::make(head, 0, 0));
+            }
         }
     }
 }
@@ -277,26 +312,38 @@ __device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uin
 {
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t n = (w << 5) + lane;
-        const bool ok = n < g.N;
-        uint32_t r = 0;
-        if (ok) {
-            const uint32_t p = WT::parent(t.uf.ld(n));
-            r = WT::parent(t.uf.ld(p));
-            if (r != p) t.uf.st(n, WT::make(r, 0, 0));
-        }
+    // Two words per iteration (w0 and w1 = w0 + nwarps) keep two independent
+    // chains of loads in flight.
+    for (uint32_t w0 = warp; w0 < g.NW; w0 += 2u * nwarps) {
+        const uint32_t w1 = w0 + nwarps;
+        const uint32_t n0 = (w0 << 5) + lane, n1 = (w1 << 5) + lane;
+        const bool ok0 = n0 < g.N, ok1 = n1 < g.N;
+        uint32_t r0 = 0, r1 = 0, p0 = 0, p1 = 0;
+        if (ok0) p0 = WT::parent(t.uf.ld(n0));
+        if (ok1) p1 = WT::parent(t.uf.ld(n1));
+        if (ok0) r0 = WT::parent(t.uf.ld(p0));
+        if (ok1) r1 = WT::parent(t.uf.ld(p1));
+        if (ok0 && r0 != p0) t.uf.st(n0, WT::make(r0, 0, 0));
+        if (ok1 && r1 != p1) t.uf.st(n1, WT::make(r1, 0, 0));
         if (flip) {
-            const uint32_t fl = ok ? (t.FLIP[r >> 5] >> (r & 31u)) & 1u : 0u;
-            const uint32_t s = t.S[w];
-            const uint32_t ns = __ballot_sync(0xFFFFFFFFu, ok && (((s >> lane) & 1u) ^ fl)) & g.valid(w);
-            if (lane == 0) t.S[w] = ns;
+            const uint32_t f0 = ok0 ? (t.FLIP[r0 >> 5] >> (r0 & 31u)) & 1u : 0u;
+            const uint32_t f1 = ok1 ? (t.FLIP[r1 >> 5] >> (r1 & 31u)) & 1u : 0u;
+            const uint32_t s0 = t.S[w0], s1 = w1 < g.NW ? t.S[w1] : 0u;
+            const uint32_t ns0 = __ballot_sync(0xFFFFFFFFu, ok0 && (((s0 >> lane) & 1u) ^ f0)) & g.valid(w0);
+            const uint32_t ns1 = __ballot_sync(0xFFFFFFFFu, ok1 && (((s1 >> lane) & 1u) ^ f1));
+            if (lane == 0) t.S[w0] = ns0;
+            if (lane == 1 && w1 < g.NW) t.S[w1] = ns1 & g.valid(w1);
         }
         if (count) {
-            const uint32_t live = __ballot_sync(0xFFFFFFFFu, ok);
-            if (ok) {
-                const uint32_t grp = __match_any_sync(live, r);
-                if (lane == (uint32_t)(__ffs(grp) - 1)) t.uf.add(r, WT::count_inc(__popc(grp)));
+            const uint32_t live0 = __ballot_sync(0xFFFFFFFFu, ok0);
+            if (ok0) {
+                const uint32_t grp = __match_any_sync(live0, r0);
+                if (lane == (uint32_t)(__ffs(grp) - 1)) t.uf.add(r0, WT::count_inc(__popc(grp)));
+            }
+            const uint32_t live1 = __ballot_sync(0xFFFFFFFFu, ok1);
+            if (ok1) {
+                const uint32_t grp = __match_any_sync(live1, r1);
+                if (lane == (uint32_t)(__ffs(grp) - 1)) t.uf.add(r1, WT::count_inc(__popc(grp)));
             }
         }
     }

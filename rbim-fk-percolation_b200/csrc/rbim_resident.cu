@@ -548,9 +548,17 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t v)
     return v;
 }
 
+// Run pieces: the sites of a word split into maximal runs of occupied
+// y-bonds; every piece starts at a run head or at bit 0 of the word and all
+// its sites share one root.  Bits of the pieces' first sites.
+__device__ __forceinline__ uint32_t piece_leaders(const Lat<Word16> &t, uint32_t w, uint32_t valid)
+{
+    return (head_mask(t.OV, w, valid) | 1u) & valid;
+}
+
 // The labelling stages shared by the sweep and label kernels, from occupied
 // bond planes to final roots; barriers between stages.  Returns the number of
-// roots counted by this warp.
+// roots counted by this warp.  Afterwards every site's word holds its root.
 template <int NT>
 __device__ __forceinline__ uint32_t resident_label(const Res &r, bool flip)
 {
@@ -639,11 +647,11 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             red.downs_t = d;
         }
     }
-    // Cluster sizes into the root words: one add per piece of run inside a
-    // word (a run shares its root), made by the piece's first site.
+    // Cluster sizes into the root words: one add per run piece (the sites of
+    // a word split into maximal runs share a root), made by its first site.
     for (uint32_t w = warp; w < g.NW; w += nwarps) {
         const uint32_t valid = g.valid(w);
-        const uint32_t lead = (head_mask(t.OV, w, valid) | 1u) & valid;
+        const uint32_t lead = piece_leaders(t, w, valid);
         if ((lead >> lane) & 1u) {
             const uint32_t n = (w << 5) + lane;
             const uint32_t next = lead & ~mask_le(lane);
