@@ -23,11 +23,19 @@
  * order (2*L*L per lattice, bond 2n horizontal, 2n+1 vertical).
  *
  * Random numbers: Philox4x32-10 keyed by the chain key, counter
- * {block, sweep_lo, sweep_hi, stream}; stream 0 bonds (bond k -> word k&3 of
- * block k>>2), stream 1 cluster flips (root r -> bit r&127 of block r>>7),
- * stream 2 hot-start spins (site n -> bit n&127 of block n>>7, sweep 0).
- * A bond is occupied iff satisfied and its word < thr, where
- * thr = floor((1 - exp(-2/T)) * 2^32) (0 <= thr <= 2^32).
+ * {block, sweep_lo, sweep_hi, stream}.
+ *   stream 0, bonds: site n (chunk c = n >> 7, row s = (n >> 5) & 3, lane
+ *     i = n & 31) reads word s of block 32*c + i; its low 16 bits draw the
+ *     horizontal bond 2n, its high 16 bits the vertical bond 2n+1.
+ *   stream 3, bond refinement: the same half of the same word of stream 3
+ *     supplies the low 16 bits of a bond's 32-bit uniform, read only when the
+ *     16-bit draw u equals thr >> 16; the uniform is (u << 16) | v.
+ *   stream 1, cluster flips: the cluster whose smallest site is r flips iff
+ *     bit r & 127 of block r >> 7 is set.
+ *   stream 2, hot-start spins: site n is -1 iff bit n & 127 of block n >> 7
+ *     (sweep 0) is set.
+ * A bond is occupied iff satisfied (J s_i s_j = +1) and its 32-bit uniform is
+ * < thr, where thr = floor((1 - exp(-2/T)) * 2^32) (0 <= thr <= 2^32).
  */
 #ifndef RBIM_SM100_H
 #define RBIM_SM100_H
