@@ -172,6 +172,36 @@ int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const
                       double *acc_f64, int32_t *records, int n_sweeps, int32_t *status, void *workspace,
                       size_t workspace_bytes, void *stream);
 
+/*
+ * rbim_sweeps_plain without a caller workspace.  No counterpart in the
+ * reference (its sweep is numba on the host); this is an addition for callers
+ * that cannot allocate device memory: an FFI host that holds only the data
+ * buffers another runtime handed it and no device allocator of its own, or a
+ * caller whose device memory is all reserved by a pooling allocator, where a
+ * cudaMalloc would fail (and a cudaFree would synchronise the device).
+ *
+ * Same arguments, results and accumulator/record contract as
+ * rbim_sweeps_plain, minus workspace and workspace_bytes: the scratch is one
+ * static device array of 2.25 MiB per device inside the library, enough for
+ * L <= RBIM_NOALLOC_MAX_L.  Larger L is rejected with RBIM_ERR_UNSUPPORTED
+ * and a message naming the limit.  Nothing is allocated, by the library or
+ * by any library it calls.
+ *
+ * The first call on each device (the device current on the calling thread)
+ * does the set-up: it looks up the array's device address with
+ * cudaGetSymbolAddress and caches it; make that first call before any stream
+ * capture begins.  Nothing has to start at zero: the call initialises every
+ * part of the scratch it reads.  The scratch is shared by all calls on a
+ * device, so two calls that overlap on the device (different streams, or
+ * different host threads, without ordering between them) race on it and give
+ * wrong results; order them on one stream or serialise them.
+ */
+#define RBIM_NOALLOC_MAX_L 512
+int rbim_noalloc_max_l(void);
+int rbim_sweeps_plain_noalloc(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                              int64_t *acc_int, double *acc_f64, int32_t *records, int n_sweeps, int32_t *status,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

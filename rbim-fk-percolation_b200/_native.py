@@ -65,6 +65,8 @@ EXPORTED_SYMBOLS = (
     "rbim_sweeps_batched",
     "rbim_plain_workspace_bytes",
     "rbim_sweeps_plain",
+    "rbim_noalloc_max_l",
+    "rbim_sweeps_plain_noalloc",
 )
 
 
@@ -104,6 +106,10 @@ def _declare(l):
     l.rbim_plain_workspace_bytes.argtypes = [c_i64]
     l.rbim_sweeps_plain.restype = c_int
     l.rbim_sweeps_plain.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p, c_size, p]
+    l.rbim_noalloc_max_l.restype = c_int
+    l.rbim_noalloc_max_l.argtypes = []
+    l.rbim_sweeps_plain_noalloc.restype = c_int
+    l.rbim_sweeps_plain_noalloc.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p]
 
 
 def lib(build_if_missing: bool = True):

@@ -2,6 +2,7 @@
 // error reporting and dispatch to the resident and plain engines.
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "rbim_internal.h"
@@ -225,6 +226,86 @@ int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const
     cudaError_t e = rbim::launch_plain_sweeps(chain, spin_pool, coupling_pool, (long long *)acc_int, acc_f64,
                                               records, n_sweeps, status, workspace, L, (cudaStream_t)stream);
     return cuda_check(e, "rbim_sweeps_plain");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Plain sweeps with a static device scratch (rbim_sweeps_plain_noalloc).
+//
+// The plain engine's workspace for L <= RBIM_NOALLOC_MAX_L lives in one
+// file-scope device array, so the entry point needs no caller workspace and
+// allocates nothing.  Its device address is looked up once per device with
+// cudaGetSymbolAddress on the first call made with that device current.
+// The scratch needs no clearing by anyone: every part of it the sweep reads
+// is written earlier in the same call (k_plain_begin zeroes the seam plane
+// and the scalar block, the phases rewrite the union-find words and the bit
+// planes every sweep), exactly as for the caller-provided workspace of
+// rbim_sweeps_plain, which may hold arbitrary bytes.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocMaxL = RBIM_NOALLOC_MAX_L;
+// 2.25 MiB; rbim::plain_workspace_bytes(512) is 2,295,296 bytes.
+constexpr size_t kNoAllocScratchBytes = size_t(2304) * 1024;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device (set-up on first use).
+int noalloc_scratch(void **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_check(e, "rbim_sweeps_plain_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(RBIM_ERR_UNSUPPORTED, "rbim_sweeps_plain_noalloc: device index %d >= %d", dev,
+                    kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_check(e, "rbim_sweeps_plain_noalloc: cudaGetSymbolAddress");
+        if (!p || ((uintptr_t)p & 255u) != 0)
+            return fail(RBIM_ERR_CUDA, "rbim_sweeps_plain_noalloc: scratch address %p is not 256-byte aligned", p);
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return RBIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rbim_noalloc_max_l(void) { return (int)kNoAllocMaxL; }
+
+int rbim_sweeps_plain_noalloc(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                              int64_t *acc_int, double *acc_f64, int32_t *records, int n_sweeps, int32_t *status,
+                              void *stream)
+{
+    if (L < 3) return fail(RBIM_ERR_INVALID, "L must be at least 3 (got %lld)", (long long)L);
+    if (L > kNoAllocMaxL)
+        return fail(RBIM_ERR_UNSUPPORTED,
+                    "rbim_sweeps_plain_noalloc: L = %lld exceeds the static scratch limit L <= %lld; use "
+                    "rbim_sweeps_plain with a caller workspace",
+                    (long long)L, (long long)kNoAllocMaxL);
+    const size_t need = rbim::plain_workspace_bytes(L);
+    if (need > kNoAllocScratchBytes)
+        return fail(RBIM_ERR_UNSUPPORTED, "rbim_sweeps_plain_noalloc: L = %lld needs %zu scratch bytes > %zu",
+                    (long long)L, need, kNoAllocScratchBytes);
+    if (n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_sweeps must be >= 0");
+    if (n_sweeps == 0) return RBIM_OK;
+    if (!chain || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    void *scratch = nullptr;
+    if (int rc = noalloc_scratch(&scratch)) return rc;
+    cudaError_t e = rbim::launch_plain_sweeps(chain, spin_pool, coupling_pool, (long long *)acc_int, acc_f64,
+                                              records, n_sweeps, status, scratch, L, (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_plain_noalloc");
 }
 
 }  // extern "C"

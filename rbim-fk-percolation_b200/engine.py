@@ -230,6 +230,25 @@ class ChainSet:
                 _native.check(rc, "rbim_sweeps_plain")
                 self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
 
+    def run_plain_noalloc(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> None:
+        """As :meth:`run_plain`, through ``rbim_sweeps_plain_noalloc`` (library-static scratch, L <= 512).
+
+        Calls on one device share the scratch, so they are issued in order on
+        this set's stream.
+        """
+        if n_sweeps <= 0:
+            return
+        idx = range(self.n) if chains is None else chains
+        with _torch().cuda.device(self.device):
+            for i in idx:
+                rc = self.lib.rbim_sweeps_plain_noalloc(
+                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * i), self._ptr(self.spin_pool),
+                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
+                    self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
+                    self._ptr(self.status), self._stream())
+                _native.check(rc, "rbim_sweeps_plain_noalloc")
+                self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
+
     def remaining(self) -> int:
         """Sweeps still to run for the longest chain (host bookkeeping)."""
         return int(np.max(self.n_total - self._sweep_host))
