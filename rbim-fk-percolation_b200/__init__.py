@@ -41,14 +41,19 @@ from .simulation import (
     OBSERVABLES,
     PRIMITIVES,
     RealizationResult,
+    ScanPlan,
+    assemble_scan,
     combine_realizations,
     derive_observables,
     load_results,
     realization_from_sums,
+    plan_temperature_scan,
+    run_scan_tasks,
     run_single_realization,
     run_temperature_scan,
     save_results,
 )
+from .sharding import gather_task_sums, run_temperature_scan_sharded, shard_bounds
 from .swendsen_wang import SweepResult, aligned_spins, energy, initial_spins, magnetization, random_spins, sw_sweep
 
 __version__ = "0.1.0"
@@ -88,6 +93,13 @@ __all__ = [
     "combine_realizations",
     "run_single_realization",
     "run_temperature_scan",
+    "ScanPlan",
+    "plan_temperature_scan",
+    "run_scan_tasks",
+    "assemble_scan",
+    "shard_bounds",
+    "gather_task_sums",
+    "run_temperature_scan_sharded",
     "save_results",
     "load_results",
     "ChainSet",

@@ -33,6 +33,10 @@ __all__ = [
     "combine_realizations",
     "run_single_realization",
     "run_temperature_scan",
+    "ScanPlan",
+    "plan_temperature_scan",
+    "run_scan_tasks",
+    "assemble_scan",
     "save_results",
     "load_results",
 ]
@@ -255,19 +259,49 @@ def run_single_realization(L: int, J: np.ndarray, temperature: float, *, n_sweep
     return realization_from_sums(ib, fb, spb, measure_percolation)
 
 
-def run_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_realizations: int = 1,
-                         n_sweeps: int = 10_000, n_therm: Optional[int] = None, n_bins: int = 10, seed: int = 0,
-                         n_workers: Optional[int] = None, measure_percolation: bool = True, start: str = "hot",
-                         disorder: Optional[Iterable[tuple]] = None, engine: str = "auto", device=None,
-                         chunk: int = 1000) -> Dict[str, object]:
-    """Scan temperatures, averaging over disorder realizations (reference ``simulation.py:336-444``).
+@dataclass
+class ScanPlan:
+    """Everything a temperature scan computes before any sweep: tasks, keys, couplings, run lengths.
 
-    Same arguments, seeding, realizations and return value as the reference.
-    ``n_workers`` is accepted for compatibility and ignored: all
-    ``len(temperatures) * n_realizations`` tasks run as chains of one GPU
-    batch.  Extra keywords: ``engine`` (see :func:`run_single_realization`),
-    ``device`` and ``chunk`` (sweeps per engine call).
+    Task ``k`` is temperature ``k // n_realizations`` and realization
+    ``k % n_realizations``, the reference's T-major order
+    (``simulation.py:384-399``); ``keys[k]`` is the Philox key drawn from that
+    task's ``SeedSequence`` child.
     """
+
+    L: int
+    p: float
+    temperatures: list
+    couplings: list
+    keys: np.ndarray
+    n_sweeps: int
+    n_therm: int
+    n_bins: int
+    sweeps_per_bin: int
+    seed: int
+    hot: bool
+    start: str
+    measure_percolation: bool
+
+    @property
+    def n_realizations(self) -> int:
+        return len(self.couplings)
+
+    @property
+    def n_tasks(self) -> int:
+        return len(self.temperatures) * len(self.couplings)
+
+    def spec(self, k: int) -> ChainSpec:
+        t_index, r = divmod(k, self.n_realizations)
+        return ChainSpec(L=self.L, realization=r, key=int(self.keys[k]), beta=1.0 / self.temperatures[t_index],
+                         n_therm=self.n_therm, n_bins=self.n_bins, sweeps_per_bin=self.sweeps_per_bin)
+
+
+def plan_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_realizations: int = 1,
+                          n_sweeps: int = 10_000, n_therm: Optional[int] = None, n_bins: int = 10, seed: int = 0,
+                          measure_percolation: bool = True, start: str = "hot",
+                          disorder: Optional[Iterable[tuple]] = None) -> ScanPlan:
+    """Argument checks, disorder and per-task keys of a scan (reference ``simulation.py:362-399``)."""
     temperatures = [float(t) for t in temperatures]
     if n_therm is None:
         n_therm = max(1, n_sweeps // 10)
@@ -288,29 +322,48 @@ def run_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_r
                 f"only {len(realizations)} disorder realizations supplied but n_realizations={n_realizations}"
             )
     couplings = [couplings_from_disorder(J_h, J_v) for J_h, J_v in realizations]
-    n_r = len(couplings)
     for J in couplings:
         if J.size != 2 * L * L:
             raise ValueError(f"disorder realization has {J.size // 2} sites, expected {L * L}")
+    children = run_seeds.spawn(len(temperatures) * len(couplings))
+    keys = np.array([chain_key(c) for c in children], dtype=np.uint64)
+    return ScanPlan(L=L, p=p, temperatures=temperatures, couplings=couplings, keys=keys, n_sweeps=n_sweeps,
+                    n_therm=n_therm, n_bins=n_bins, sweeps_per_bin=spb, seed=seed, hot=hot, start=start,
+                    measure_percolation=measure_percolation)
 
-    n_tasks = len(temperatures) * n_r
-    children = run_seeds.spawn(n_tasks)
-    specs = []
-    for k in range(n_tasks):
-        t_index, r = divmod(k, n_r)
-        specs.append(ChainSpec(L=L, realization=r, key=chain_key(children[k]), beta=1.0 / temperatures[t_index],
-                               n_therm=n_therm, n_bins=n_bins, sweeps_per_bin=spb))
-    raw = []
-    if n_tasks:
-        cs = ChainSet(specs, [pack_couplings(J, L) for J in couplings], device=device)
-        cs.init_spins(hot)
-        cs.run_to_end(engine=engine, chunk=chunk)
-        acc_i, acc_f = cs.all_bins()
-        for k in range(n_tasks):
-            a = cs.acc_off[k]
-            raw.append(realization_from_sums(acc_i[a: a + n_bins], acc_f[a: a + n_bins], spb, measure_percolation))
 
-    n_sites = L * L
+def run_scan_tasks(plan: ScanPlan, tasks: Optional[Sequence[int]] = None, *, engine: str = "auto", device=None,
+                   chunk: int = 1000):
+    """Run some tasks of a plan on one GPU; returns their per-bin sums.
+
+    ``(int_sums, f64_sums)`` with shapes ``(len(tasks), n_bins, 12)`` int64
+    and ``(len(tasks), n_bins, 2)`` float64.  A task's sums do not depend on
+    which other tasks share the batch.
+    """
+    tasks = list(range(plan.n_tasks)) if tasks is None else [int(k) for k in tasks]
+    nb = plan.n_bins
+    int_sums = np.zeros((len(tasks), nb, 12), dtype=np.int64)
+    f_sums = np.zeros((len(tasks), nb, 2), dtype=np.float64)
+    if not tasks:
+        return int_sums, f_sums
+    cs = ChainSet([plan.spec(k) for k in tasks], [pack_couplings(J, plan.L) for J in plan.couplings], device=device)
+    cs.init_spins(plan.hot)
+    cs.run_to_end(engine=engine, chunk=chunk)
+    acc_i, acc_f = cs.all_bins()
+    for i in range(len(tasks)):
+        a = cs.acc_off[i]
+        int_sums[i] = acc_i[a: a + nb]
+        f_sums[i] = acc_f[a: a + nb]
+    return int_sums, f_sums
+
+
+def assemble_scan(plan: ScanPlan, int_sums: np.ndarray, f_sums: np.ndarray) -> Dict[str, object]:
+    """Jackknife-combined observables and metadata from every task's sums (reference ``simulation.py:401-444``)."""
+    n_r = plan.n_realizations
+    temperatures = plan.temperatures
+    raw = [realization_from_sums(int_sums[k], f_sums[k], plan.sweeps_per_bin, plan.measure_percolation)
+           for k in range(plan.n_tasks)]
+    n_sites = plan.L * plan.L
     results = {name: {"value": np.empty(len(temperatures)), "error": np.empty(len(temperatures)),
                       "thermal_error": np.empty(len(temperatures))} for name in OBSERVABLES}
     for t_index, temperature in enumerate(temperatures):
@@ -321,15 +374,15 @@ def run_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_r
                 results[name][key][t_index] = combined[name][key]
 
     metadata = {
-        "L": L,
-        "p": p,
+        "L": plan.L,
+        "p": plan.p,
         "n_realizations": n_r,
-        "n_sweeps": n_sweeps,
-        "n_therm": n_therm,
-        "n_bins": n_bins,
-        "seed": seed,
-        "measure_percolation": measure_percolation,
-        "start": start,
+        "n_sweeps": plan.n_sweeps,
+        "n_therm": plan.n_therm,
+        "n_bins": plan.n_bins,
+        "seed": plan.seed,
+        "measure_percolation": plan.measure_percolation,
+        "start": plan.start,
         "algorithm": "Swendsen-Wang cluster update on satisfied bonds",
         "estimator": (
             "primitive moments accumulated over the full run of each realization; "
@@ -347,6 +400,26 @@ def run_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_r
         "rng": "philox4x32-10 per chain (key from the task's SeedSequence child)",
     }
     return {"temperatures": np.asarray(temperatures), "observables": results, "metadata": metadata}
+
+
+def run_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_realizations: int = 1,
+                         n_sweeps: int = 10_000, n_therm: Optional[int] = None, n_bins: int = 10, seed: int = 0,
+                         n_workers: Optional[int] = None, measure_percolation: bool = True, start: str = "hot",
+                         disorder: Optional[Iterable[tuple]] = None, engine: str = "auto", device=None,
+                         chunk: int = 1000) -> Dict[str, object]:
+    """Scan temperatures, averaging over disorder realizations (reference ``simulation.py:336-444``).
+
+    Same arguments, seeding, realizations and return value as the reference.
+    ``n_workers`` is accepted for compatibility and ignored: all
+    ``len(temperatures) * n_realizations`` tasks run as chains of one GPU
+    batch.  Extra keywords: ``engine`` (see :func:`run_single_realization`),
+    ``device`` and ``chunk`` (sweeps per engine call).
+    """
+    plan = plan_temperature_scan(L, p, temperatures, n_realizations=n_realizations, n_sweeps=n_sweeps,
+                                 n_therm=n_therm, n_bins=n_bins, seed=seed, measure_percolation=measure_percolation,
+                                 start=start, disorder=disorder)
+    int_sums, f_sums = run_scan_tasks(plan, engine=engine, device=device, chunk=chunk)
+    return assemble_scan(plan, int_sums, f_sums)
 
 
 def save_results(path: str, results: Dict[str, object]) -> None:
