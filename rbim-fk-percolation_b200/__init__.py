@@ -53,6 +53,7 @@ from .simulation import (
     run_temperature_scan,
     save_results,
 )
+from .serving import RangeAllocator, ScanRequest, ScanServer, request_footprint
 from .sharding import gather_task_sums, run_temperature_scan_sharded, shard_bounds
 from .swendsen_wang import SweepResult, aligned_spins, energy, initial_spins, magnetization, random_spins, sw_sweep
 
@@ -100,6 +101,10 @@ __all__ = [
     "shard_bounds",
     "gather_task_sums",
     "run_temperature_scan_sharded",
+    "ScanRequest",
+    "ScanServer",
+    "RangeAllocator",
+    "request_footprint",
     "save_results",
     "load_results",
     "ChainSet",
