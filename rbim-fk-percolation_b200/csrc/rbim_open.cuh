@@ -1,0 +1,283 @@
+// Open-lattice labelling on a 16-bit shared-memory union-find, shared by the
+// resident engine (one lattice per CTA) and the cluster engine (one tile of a
+// lattice per CTA).  Inside an open region of the lattice (no bond that
+// crosses a periodic seam) every cycle is contractible, so the union-find
+// words carry parents only and each open cluster's root is its smallest site.
+//
+// A lattice context here is a Lat<Word16> whose Geom covers the sites held by
+// the CTA; sites whose x-bond leaves that range (the last L sites) are left to
+// the caller's seam or boundary stage.
+#pragma once
+
+#include "rbim_phases.cuh"
+
+#ifndef RBIM_COUNT
+#define RBIM_COUNT(k, v) ((void)0)
+#define RBIM_PROF_ONLY(...)
+#endif
+
+namespace rbim {
+
+// Open-lattice union-find word: the parent site only.
+struct Word16 {
+    using T = unsigned short;
+    __device__ __forceinline__ static uint32_t parent(T w) { return w; }
+    __device__ __forceinline__ static int ox(T) { return 0; }
+    __device__ __forceinline__ static int oy(T) { return 0; }
+    __device__ __forceinline__ static T make(uint32_t p, int, int) { return (T)p; }
+    __device__ __forceinline__ static T count_inc(uint32_t c) { return (T)c; }
+};
+
+// The open union-find lives in shared memory: access it through 32-bit
+// shared-window addresses with explicit ld/st/atom.shared instructions.
+template <>
+struct UF<Word16> {
+    using T = unsigned short;
+    T *w;          // generic pointer (for code that indexes the array directly)
+    uint32_t sa;   // shared-window address of w
+    __device__ __forceinline__ T ld(uint32_t i) const
+    {
+        T v;
+        asm volatile("ld.volatile.shared.u16 %0, [%1];" : "=h"(v) : "r"(sa + 2u * i) : "memory");
+        return v;
+    }
+    __device__ __forceinline__ void st(uint32_t i, T v) const
+    {
+        asm volatile("st.volatile.shared.u16 [%0], %1;" ::"r"(sa + 2u * i), "h"(v) : "memory");
+    }
+    __device__ __forceinline__ T cas(uint32_t i, T expect, T v) const
+    {
+        T old;
+        asm volatile("atom.shared.cas.b16 %0, [%1], %2, %3;"
+                     : "=h"(old)
+                     : "r"(sa + 2u * i), "h"(expect), "h"(v)
+                     : "memory");
+        return old;
+    }
+    __device__ __forceinline__ void add(uint32_t i, T v) const { uf_atomic_add(w + i, v); }
+};
+
+// Mask of the bits of word w whose site lies in the last row (x = L-1): the
+// horizontal bonds there close the x boundary.
+__device__ __forceinline__ uint32_t last_row_mask(const Geom &g, uint32_t w)
+{
+    const uint32_t n0 = w << 5, first = g.N - g.L;
+    if (n0 + 32u <= first) return 0u;
+    const uint32_t v = g.valid(w);
+    if (n0 >= first) return v;
+    return ~((1u << (first - n0)) - 1u) & v;
+}
+
+// Work slices.  Pointer chasing has data-dependent length, so the union and
+// root phases run as flat per-thread loops that take one pointer step per
+// iteration and fetch the next item as soon as the current one is done; a
+// thread's cost is then the sum of its items' steps rather than a per-round
+// maximum over the warp.  Thread t owns the bit ranges t, t + T, t + 2T, ...
+// where each word is cut into `seg` equal ranges (seg is a power of two
+// chosen so that small lattices still give every thread work).
+struct Slices {
+    uint32_t seg_log2, bits, items;
+    __device__ __forceinline__ uint32_t word(uint32_t i) const { return i >> seg_log2; }
+    __device__ __forceinline__ uint32_t mask(uint32_t i) const
+    {
+        const uint32_t s = i & ((1u << seg_log2) - 1u);
+        return (bits == 32u ? 0xFFFFFFFFu : ((1u << bits) - 1u)) << (s * bits);
+    }
+};
+
+__device__ __forceinline__ Slices make_slices(uint32_t NW, uint32_t nthreads)
+{
+    uint32_t lg = 0;
+    while (lg < 5u && (NW << (lg + 1u)) <= nthreads) ++lg;
+    return Slices{lg, 32u >> lg, NW << lg};
+}
+
+// Occupied x-bonds of word w that need a union: off the x seam, and not
+// already connected through an elementary plaquette with the bond before.
+__device__ __forceinline__ uint32_t union_need(const Lat<Word16> &t, uint32_t w)
+{
+    const Geom &g = t.g;
+    const uint32_t oh = t.OH[w] & ~last_row_mask(g, w);
+    if (!oh) return 0u;
+    Plane OVp{t.OV};
+    const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
+    const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
+    const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
+    const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
+    uint32_t s = (w << 5) + g.L - 1u;
+    if (s >= g.N) s -= g.N;
+    return oh & ~(prev_oh & prev_ov & extract32(OVp, s, g));
+}
+
+// One path-halving step of a walk at x, without branches: returns the next
+// position and sets `done` when x's parent or grandparent is the root (the
+// returned position is then the root).
+__device__ __forceinline__ uint32_t halving_step(const UF<Word16> &uf, uint32_t x, bool &done)
+{
+    const uint32_t p = uf.ld(x);
+    const uint32_t gp = uf.ld(p);
+    const bool x_root = p == x, p_root = gp == p;
+    if (!x_root && !p_root) uf.st(x, (unsigned short)gp);
+    done = x_root || p_root;
+    return x_root ? x : (p_root ? p : gp);
+}
+
+// (b) Open-lattice unions across occupied x-bonds that do not cross the x
+// seam: the larger root is hooked under the smaller with a 16-bit CAS, finds
+// use path halving, and a union whose CAS loses a race restarts from the two
+// roots it found.  Both endpoint walks advance in the same loop iteration.
+__device__ __forceinline__ void phase_union_open(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
+{
+    const Geom &g = t.g;
+    const UF<Word16> &uf = t.uf;
+    const Slices sl = make_slices(g.NW, nthreads);
+    uint32_t item = tid, pending = 0, base = 0;
+    uint32_t xa = 0, xb = 0;
+    bool fetch = true;
+    const uint32_t cap = 64u * g.N + 4096u;
+    uint32_t it = 0;
+    RBIM_PROF_ONLY(uint32_t n_bonds = 0; uint32_t n_fails = 0);
+    for (;; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrUnionCap);
+            break;
+        }
+        if (fetch) {
+            while (!pending && item < sl.items) {
+                const uint32_t w = sl.word(item);
+                pending = union_need(t, w) & sl.mask(item);
+                base = w << 5;
+                item += nthreads;
+            }
+            if (!pending) break;
+            xa = base + (uint32_t)(__ffs(pending) - 1);
+            pending &= pending - 1u;
+            xb = xa + g.L;
+            fetch = false;
+            RBIM_PROF_ONLY(++n_bonds);
+        }
+        bool da, db;
+        xa = halving_step(uf, xa, da);
+        xb = halving_step(uf, xb, db);
+        if (da && db) {
+            // Both walks are at roots.
+            if (xa == xb) {
+                fetch = true;
+            } else {
+                const uint32_t lo = min(xa, xb), hi = max(xa, xb);
+                fetch = uf.cas(hi, (unsigned short)hi, (unsigned short)lo) == (unsigned short)hi;
+                // A lost race leaves both walks at their old roots, to resume from.
+                RBIM_PROF_ONLY(n_fails += fetch ? 0u : 1u);
+            }
+        }
+    }
+#ifdef RBIM_PROFILE_PHASES
+    {
+        uint32_t mx = it, sm = it;
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+            sm += __shfl_xor_sync(0xFFFFFFFFu, sm, o);
+        }
+        uint32_t nb = n_bonds, nf = n_fails;
+        for (int o = 16; o > 0; o >>= 1) {
+            nb += __shfl_xor_sync(0xFFFFFFFFu, nb, o);
+            nf += __shfl_xor_sync(0xFFFFFFFFu, nf, o);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            RBIM_COUNT(3, mx);
+            RBIM_COUNT(4, sm);
+            RBIM_COUNT(0, nb);
+            RBIM_COUNT(2, nf);
+        }
+    }
+#endif
+}
+
+// (c) Roots of the run heads (see phase_roots), as a flat per-thread loop
+// over the heads of the thread's slices: read-only walks, each head's final
+// root written by the head's own thread.  ROOT must be zero on entry.
+// Returns the number of roots this thread found.
+// Next head of the thread's slices into (h, x), or false when there is none.
+__device__ __forceinline__ bool next_head(const Lat<Word16> &t, const Slices &sl, uint32_t nthreads, uint32_t &item,
+                                          uint32_t &pending, uint32_t &base, uint32_t &h)
+{
+    while (!pending && item < sl.items) {
+        const uint32_t w = sl.word(item);
+        pending = head_mask(t.OV, w, t.g.valid(w)) & sl.mask(item);
+        base = w << 5;
+        item += nthreads;
+    }
+    if (!pending) return false;
+    h = base + (uint32_t)(__ffs(pending) - 1);
+    pending &= pending - 1u;
+    return true;
+}
+
+__device__ __forceinline__ uint32_t phase_roots_flat(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
+{
+    const Geom &g = t.g;
+    const Slices sl = make_slices(g.NW, nthreads);
+    uint32_t item = tid, pending = 0, base = 0, nroots = 0;
+    // Two walks in flight per thread: heads h0, h1 at positions x0, x1.
+    uint32_t h0 = 0, h1 = 0, x0 = 0, x1 = 0;
+    bool a0 = next_head(t, sl, nthreads, item, pending, base, h0);
+    bool a1 = a0 && next_head(t, sl, nthreads, item, pending, base, h1);
+    x0 = h0;
+    x1 = h1;
+    const uint32_t cap = 64u * g.N + 4096u;
+    for (uint32_t it = 0; a0 || a1; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrFindCap);
+            break;
+        }
+        const uint32_t p0 = t.uf.ld(x0), p1 = t.uf.ld(x1);
+        const bool r0 = a0 && p0 == x0, r1 = a1 && p1 == x1;
+        x0 = p0;
+        x1 = p1;
+        if (r0) {
+            if (x0 != h0) {
+                t.uf.st(h0, (unsigned short)x0);
+            } else {
+                atomicOr(t.ROOT + (h0 >> 5), 1u << (h0 & 31u));
+                ++nroots;
+            }
+            a0 = next_head(t, sl, nthreads, item, pending, base, h0);
+            x0 = h0;
+        }
+        if (r1) {
+            if (x1 != h1) {
+                t.uf.st(h1, (unsigned short)x1);
+            } else {
+                atomicOr(t.ROOT + (h1 >> 5), 1u << (h1 & 31u));
+                ++nroots;
+            }
+            a1 = next_head(t, sl, nthreads, item, pending, base, h1);
+            x1 = h1;
+        }
+    }
+    return nroots;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// Run pieces: the sites of a word split into maximal runs of occupied
+// y-bonds; every piece starts at a run head or at bit 0 of the word and all
+// its sites share one root.  Bits of the pieces' first sites.
+__device__ __forceinline__ uint32_t piece_leaders(const Lat<Word16> &t, uint32_t w, uint32_t valid)
+{
+    return (head_mask(t.OV, w, valid) | 1u) & valid;
+}
+
+// Add v to the 16-bit word i through its 32-bit container (no carry can
+// leave the half: cluster sizes stay below 65536 whenever counts are taken).
+__device__ __forceinline__ void add16(unsigned short *base, uint32_t i, uint32_t v)
+{
+    atomicAdd((unsigned int *)(base + (i & ~1u)), v << (16u * (i & 1u)));
+}
+
+}  // namespace rbim
