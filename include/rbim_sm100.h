@@ -161,6 +161,23 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
                         void *stream);
 
 /*
+ * Batched sweeps of lattices too large for one CTA: every chain of `chains`
+ * (rbim_resident_max_l() < L <= l_max <= rbim_cluster_max_l()) advances by up
+ * to n_sweeps sweeps, one lattice per thread-block cluster.  The cluster's
+ * CTAs each hold one tile of at most 65536 consecutive sites in shared memory
+ * for the whole call and merge the clusters that cross tile boundaries or
+ * the periodic seams through distributed shared memory.  Same chain,
+ * accumulator and record contract (and the same results, bit for bit) as
+ * rbim_sweeps_batched; workspace: rbim_batched_workspace_bytes() bytes.
+ * rbim_cluster_max_l() depends on the current device (0 when no cluster can
+ * be scheduled).
+ */
+int rbim_cluster_max_l(void);
+int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
+                          const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
+                          int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream);
+
+/*
  * Plain sweeps of one chain (device descriptor `chain`) through the
  * global-memory engine: one lattice per launch sequence, any L >= 3, the
  * drop-in for one run_single_realization task.  L must equal chain->L.  Same

@@ -24,6 +24,7 @@ __all__ = [
     "REC_LEN",
     "plane_words",
     "resident_max_l",
+    "cluster_max_l",
     "EXPORTED_SYMBOLS",
 ]
 
@@ -65,6 +66,8 @@ EXPORTED_SYMBOLS = (
     "rbim_sweeps_batched",
     "rbim_plain_workspace_bytes",
     "rbim_sweeps_plain",
+    "rbim_cluster_max_l",
+    "rbim_sweeps_clustered",
     "rbim_noalloc_max_l",
     "rbim_sweeps_plain_noalloc",
 )
@@ -106,6 +109,10 @@ def _declare(l):
     l.rbim_plain_workspace_bytes.argtypes = [c_i64]
     l.rbim_sweeps_plain.restype = c_int
     l.rbim_sweeps_plain.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p, c_size, p]
+    l.rbim_cluster_max_l.restype = c_int
+    l.rbim_cluster_max_l.argtypes = []
+    l.rbim_sweeps_clustered.restype = c_int
+    l.rbim_sweeps_clustered.argtypes = [p, c_int, c_i64, p, p, p, p, p, c_int, p, p, c_size, p]
     l.rbim_noalloc_max_l.restype = c_int
     l.rbim_noalloc_max_l.argtypes = []
     l.rbim_sweeps_plain_noalloc.restype = c_int
@@ -152,3 +159,8 @@ def plane_words(L: int) -> int:
 def resident_max_l() -> int:
     """Largest L the on-chip engine takes (``rbim_resident_max_l``)."""
     return int(lib().rbim_resident_max_l())
+
+
+def cluster_max_l() -> int:
+    """Largest L the cluster engine takes on the current device (``rbim_cluster_max_l``; 0 if none)."""
+    return int(lib().rbim_cluster_max_l())

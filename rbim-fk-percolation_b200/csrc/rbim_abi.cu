@@ -209,6 +209,62 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
     return cuda_check(e, "rbim_sweeps_batched");
 }
 
+int rbim_cluster_max_l(void)
+{
+    // Per device: the largest L whose cluster fits the shared-memory budget
+    // and can be scheduled at least once.
+    static int cached[64];
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (cached[dev]) return cached[dev] > 0 ? cached[dev] : 0;
+    int ok_c[17] = {};  // per cluster size: 1 schedulable, -1 not
+    int best = -1;
+    for (int L = 1024; L > rbim::resident_max_l(); --L) {
+        const uint32_t C = rbim::cluster_size_for((uint32_t)L);
+        if (C == 0) continue;
+        if (!rbim::cluster_layout_fits(rbim::cluster_layout((uint32_t)L, C))) continue;
+        if (ok_c[C] == 0) {
+            int clusters = 0;
+            const cudaError_t e = rbim::cluster_occupancy((uint32_t)L, C, &clusters);
+            ok_c[C] = (e == cudaSuccess && clusters > 0) ? 1 : -1;
+            if (e != cudaSuccess) cudaGetLastError();
+        }
+        if (ok_c[C] > 0) {
+            best = L;
+            break;
+        }
+    }
+    cached[dev] = best;
+    return best > 0 ? best : 0;
+}
+
+int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
+                          const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
+                          int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (n_chains < 0 || n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_chains and n_sweeps must be >= 0");
+    if (n_chains == 0 || n_sweeps == 0) return RBIM_OK;
+    if (int rc = check_chain_sizes(l_max)) return rc;
+    if (l_max <= rbim::resident_max_l())
+        return fail(RBIM_ERR_INVALID, "l_max = %lld is small enough for rbim_sweeps_batched (limit %d)",
+                    (long long)l_max, rbim::resident_max_l());
+    if (!chains || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status || !workspace)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    if (!aligned16(spin_pool) || !aligned16(coupling_pool))
+        return fail(RBIM_ERR_INVALID, "spin and coupling pools must be 16-byte aligned");
+    if (workspace_bytes < rbim_batched_workspace_bytes()) return fail(RBIM_ERR_INVALID, "workspace too small");
+    const int lim = rbim_cluster_max_l();
+    if (l_max > lim)
+        return fail(RBIM_ERR_UNSUPPORTED, "l_max = %lld exceeds the cluster engine's limit %d on this device",
+                    (long long)l_max, lim);
+    cudaError_t e = rbim::launch_cluster_sweeps(chains, n_chains, (int)l_max, spin_pool, coupling_pool,
+                                                (long long *)acc_int, acc_f64, records, n_sweeps, (int *)workspace,
+                                                status, (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_clustered");
+}
+
 size_t rbim_plain_workspace_bytes(int64_t L) { return L < 3 ? 0 : rbim::plain_workspace_bytes(L); }
 
 int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,

@@ -1,0 +1,948 @@
+// Cluster engine: one lattice per thread-block cluster, for lattices too large
+// for one CTA (L > 256, up to 1024).  The C CTAs of a cluster split the
+// lattice into C tiles of consecutive sites (tile c holds global sites
+// [c*T, c*T + Tc), T a multiple of 128 and at most 65536), each held in its
+// CTA's shared memory for every sweep of a call, exactly like the resident
+// engine holds a whole lattice:
+//
+//  1. activation of the bonds owned by the tile's sites (the x-bond of the
+//     last L sites and the y-bond of the tile's last site reach the next
+//     tile; the spins they need are a halo copied from the neighbour CTA's
+//     shared memory through distributed shared memory);
+//  2. the open-tile labelling of the resident engine (16-bit parents, run
+//     heads, flat union and root walks): inside a tile every cycle is
+//     contractible;
+//  3. the boundary bonds -- x-bonds from the last L sites of a tile (into the
+//     next tile, or across the x seam from the last tile to the first), the
+//     y-bond between two tiles, and the y-seam bonds -- are unioned in a
+//     cluster-wide union-find over the tile roots they touch.  Its nodes live
+//     in hash tables in the CTAs' shared memory; words carry image offsets
+//     (Word64: parent node | wx | wy), and a boundary bond that closes a
+//     loop with nonzero summed offset winds around the torus (the exact test
+//     of src/rbim/_unionfind.py:104-124).  The larger key (global site of a
+//     node's tile root) is hooked under the smaller, so a merged cluster's
+//     root node is its smallest site, the canonical label that keys its flip;
+//  4. flip, halo refresh and the measurement reductions across the cluster.
+//
+// Node ids are (tile << 16) | slot; every access to another CTA's shared
+// memory goes through cluster.map_shared_rank, and every phase that reads or
+// writes another CTA's memory is fenced by cluster barriers.
+//
+// This replaces, per chain, the loop of run_single_realization
+// (src/rbim/simulation.py:196-242) around sw_sweep
+// (src/rbim/swendsen_wang.py:103-172), with the same Philox stream and
+// bit-identical results to the oracle's sweep.
+#include <algorithm>
+#include <cooperative_groups.h>
+
+#include "rbim_internal.h"
+#include "rbim_open.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace rbim {
+
+namespace {
+
+constexpr int kCT = 1024;               // threads per CTA
+constexpr uint32_t kTileMax = 65536;    // 16-bit tile parents
+constexpr uint32_t kClusterMax = 16;    // non-portable cluster size limit
+constexpr uint32_t kSlotsPerThread = 4; // hash size <= 4 * kCT
+constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr size_t kSmemBudget = 227 * 1024 - 4 * 1024;
+
+size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
+
+}  // namespace
+
+uint32_t cluster_size_for(uint32_t L)
+{
+    for (uint32_t C = 2; C <= kClusterMax; ++C)
+        if (cluster_tiles_ok(L, C)) return C;
+    return 0;
+}
+
+namespace {
+
+uint32_t cluster_hash_size(uint32_t l_max, uint32_t T)
+{
+    // Tile roots that can touch a boundary bond: the first and last L sites,
+    // the row ends and row starts of the tile's rows, the tile-end site.
+    const uint32_t rows = T / l_max + 2u;
+    const uint32_t bound = 2u * l_max + 2u * rows + 1u;
+    uint32_t h = 64;
+    while (h < bound + bound / 2u) h *= 2;
+    return h;
+}
+
+}  // namespace
+
+ClusterLayout cluster_layout(uint32_t l_max, uint32_t C)
+{
+    ClusterLayout ly{};
+    ly.l_max = l_max;
+    ly.C = C;
+    ly.t_max = cluster_tile_size(l_max * l_max, C);
+    ly.tw = ly.t_max / 32u;
+    ly.hs = cluster_hash_size(l_max, ly.t_max);
+    size_t off = 0;
+    ly.off_uf = off;
+    off = a16(off + 2ull * ly.t_max);
+    ly.off_S = off;  // tile, halo of l_max sites, padding
+    off = a16(off + 4ull * (ly.tw + (l_max + 31u) / 32u + 4u));
+    const size_t plane = a16(4ull * (ly.tw + 4u));
+    ly.off_OH = off;
+    off += plane;
+    ly.off_OV = off;
+    off += plane;
+    ly.off_FLIP = off;
+    off += plane;
+    ly.off_ROOT = off;
+    off += plane;
+    ly.off_YS = off;  // y-seam bonds, one bit per row of the tile
+    off = a16(off + 4ull * 16u);
+    ly.off_HK = off;
+    off = a16(off + 4ull * ly.hs);
+    ly.off_HW = off;
+    off += 8ull * ly.hs;
+    ly.bytes = a16(off);
+    return ly;
+}
+
+bool cluster_layout_fits(const ClusterLayout &ly)
+{
+    return ly.bytes <= kSmemBudget && ly.hs <= kSlotsPerThread * kCT && ly.t_max <= kTileMax;
+}
+
+namespace {
+
+// Shared scratch of one CTA of the cluster.
+struct CRed {
+    unsigned long long k1[32], k2[32];
+    uint32_t unsat[32], downs[32], ncl[32];
+    int mcw[32];
+    // This CTA's partial results, read by rank 0 through DSMEM.
+    unsigned long long p_k1, p_k2;
+    uint32_t p_unsat, p_downs, p_ncl;
+    int p_wrap, p_mc;
+    // Rank 0's combined results, read by the other CTAs.
+    uint32_t g1, ncl_total;
+    // Per chain / per sweep state.
+    int item, wrap, err;
+    uint32_t front, tile_end;
+    Acc acc;
+    long long cur_bin;
+    rbim_chain_t ch;
+};
+
+// Geometry of this CTA's tile of the current chain.
+struct Tile {
+    uint32_t L, N, C, c, T, b, Tc, tw, x0, f, nwp;
+};
+
+// Views of this CTA's shared memory and of the cluster's.
+struct Ctx {
+    Lat<Word16> t;
+    uint32_t *YS;
+    uint32_t *HK;
+    unsigned long long *HW;
+    uint32_t hs, hs_log2;
+};
+
+__device__ __forceinline__ Ctx make_ctx(unsigned char *smem, const ClusterLayout &ly, const Tile &tl, CRed &red)
+{
+    Ctx x;
+    Lat<Word16> &t = x.t;
+    t.g = Geom{tl.L, tl.Tc, (tl.Tc + 31u) / 32u};
+    t.uf.w = (unsigned short *)(smem + ly.off_uf);
+    t.uf.sa = (uint32_t)__cvta_generic_to_shared(t.uf.w);
+    t.S = (uint32_t *)(smem + ly.off_S);
+    t.JH = nullptr;
+    t.JV = nullptr;
+    t.OH = (uint32_t *)(smem + ly.off_OH);
+    t.OV = (uint32_t *)(smem + ly.off_OV);
+    t.FLIP = (uint32_t *)(smem + ly.off_FLIP);
+    t.ROOT = (uint32_t *)(smem + ly.off_ROOT);
+    t.RE = nullptr;
+    t.SEAMV = nullptr;
+    t.wrap = &red.wrap;
+    t.err = &red.err;
+    t.cap = tl.Tc + 64u;
+    x.YS = (uint32_t *)(smem + ly.off_YS);
+    x.HK = (uint32_t *)(smem + ly.off_HK);
+    x.HW = (unsigned long long *)(smem + ly.off_HW);
+    x.hs = ly.hs;
+    x.hs_log2 = 31u - __clz(ly.hs);
+    return x;
+}
+
+// Row-end bit of tile word w (at most one: L > 32).
+__device__ __forceinline__ uint32_t tile_row_end(const Tile &tl, uint32_t w, uint32_t valid)
+{
+    const uint32_t n0 = tl.b + (w << 5);
+    const uint32_t p = (tl.L - 1u) - (n0 % tl.L);
+    return p < 32u ? (1u << p) & valid : 0u;
+}
+
+// 32 bits of the tile's spin plane from local bit `start` (no wrap: the
+// plane holds the tile, then the halo, then zero words).
+__device__ __forceinline__ uint32_t extract_nowrap(const uint32_t *P, uint32_t start)
+{
+    const uint32_t wi = start >> 5, sh = start & 31u;
+    const uint32_t lo = P[wi];
+    return sh ? __funnelshift_r(lo, P[wi + 1u], sh) : lo;
+}
+
+// +y neighbours of tile word w: site m+1, or the row start m+1-L at a row
+// end; the row start of the tile's first (partial) row lies in the previous
+// tile and is the front spin.
+__device__ __forceinline__ uint32_t tile_ynext(const uint32_t *S, uint32_t w, uint32_t re, uint32_t L, uint32_t front)
+{
+    uint32_t r = extract_nowrap(S, (w << 5) + 1u) & ~re;
+    if (re) {
+        const uint32_t bit = __ffs(re) - 1u;
+        const int q = (int)((w << 5) + bit) + 1 - (int)L;
+        const uint32_t v = q >= 0 ? (S[(uint32_t)q >> 5] >> ((uint32_t)q & 31u)) & 1u : front;
+        r |= v << bit;
+    }
+    return r;
+}
+
+// (a) Bond activation of the tile: the resident engine's chunk scheme with
+// the chunk index offset by the tile's first chunk, so that every bond draws
+// the same Philox word as in the whole-lattice engines.  OV keeps the y-bonds
+// inside the tile; y-seam bonds go to YS (bit = row - x0), the y-bond from
+// the tile's last site into the next tile to red.tile_end.
+__device__ __forceinline__ void tile_activate(const Ctx &x, const Tile &tl, const SweepRng &rng, const uint32_t *gJH,
+                                              const uint32_t *gJV, uint32_t front, CRed &red, uint32_t warp,
+                                              uint32_t nwarps, uint32_t tid)
+{
+    const Lat<Word16> &t = x.t;
+    const Geom &g = t.g;
+    const uint32_t lane = tid & 31u;
+    const uint32_t nchunks = (g.N + 127u) >> 7;
+    const uint32_t chunk0 = tl.b >> 7;
+    const uint32_t last = tl.Tc - 1u;
+    const bool end_is_row_end = ((tl.b + tl.Tc) % tl.L) == 0u;
+    for (uint32_t c0 = warp; c0 < nchunks; c0 += 2u * nwarps) {
+        uint32_t sh[2], sv[2], re[2], wq[2];
+        U4 r[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t c = c0 + k * nwarps;
+            wq[k] = 4u * c + lane;
+            sh[k] = sv[k] = re[k] = 0;
+            if (lane < 4u && wq[k] < g.NW) {
+                const uint32_t v = g.valid(wq[k]);
+                re[k] = tile_row_end(tl, wq[k], v);
+                const uint32_t s = t.S[wq[k]];
+                sh[k] = ~(s ^ extract_nowrap(t.S, (wq[k] << 5) + tl.L) ^ gJH[wq[k]]) & v;
+                sv[k] = ~(s ^ tile_ynext(t.S, wq[k], re[k], tl.L, front) ^ gJV[wq[k]]) & v;
+            }
+            r[k] = philox_block(rng.key, 32u * (chunk0 + c) + lane, rng.sweep, kStreamBond);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t c = c0 + k * nwarps;
+            uint32_t dh[4], dv[4];
+            bool refine = false;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t w = u4_word(r[k], s);
+                const uint32_t bh = (__shfl_sync(0xFFFFFFFFu, sh[k], s) >> lane) & 1u;
+                const uint32_t bv = (__shfl_sync(0xFFFFFFFFu, sv[k], s) >> lane) & 1u;
+                dh[s] = bh ? bond_decide(rng, w & 0xFFFFu) : 0u;
+                dv[s] = bv ? bond_decide(rng, w >> 16) : 0u;
+                refine |= (dh[s] == 2u) | (dv[s] == 2u);
+            }
+            if (refine) {
+                const U4 q = philox_block(rng.key, 32u * (chunk0 + c) + lane, rng.sweep, kStreamBondLow);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const uint32_t w = u4_word(q, s);
+                    if (dh[s] == 2u) dh[s] = (w & 0xFFFFu) < rng.thr_lo ? 1u : 0u;
+                    if (dv[s] == 2u) dv[s] = (w >> 16) < rng.thr_lo ? 1u : 0u;
+                }
+            }
+            uint32_t oh = 0, ov = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
+                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
+                if (lane == (uint32_t)s) {
+                    oh = bh;
+                    ov = bv;
+                }
+            }
+            if (lane < 4u && wq[k] < g.NW) {
+                const uint32_t w = wq[k];
+                uint32_t keep = ov & ~re[k];
+                if (w == (last >> 5) && !end_is_row_end) {
+                    const uint32_t eb = 1u << (last & 31u);
+                    red.tile_end = (keep & eb) ? 1u : 0u;
+                    keep &= ~eb;
+                }
+                t.OH[w] = oh;
+                t.OV[w] = keep;
+                if (ov & re[k]) {
+                    const uint32_t bit = __ffs(re[k]) - 1u;
+                    const uint32_t row = (tl.b + (w << 5) + bit + 1u) / tl.L - 1u - tl.x0;
+                    atomicOr(x.YS + (row >> 5), 1u << (row & 31u));
+                }
+            }
+        }
+    }
+    // Flip bits: Philox block q of stream 1 covers global words 4q .. 4q+3.
+    const uint32_t nblk = (g.NW + 3u) >> 2;
+    for (uint32_t q = tid; q < nblk; q += kCT) {
+        const U4 rr = philox_block(rng.key, chunk0 + q, rng.sweep, kStreamFlip);
+        const uint32_t w = 4u * q;
+        t.FLIP[w] = rr.x;
+        if (w + 1u < g.NW) t.FLIP[w + 1u] = rr.y;
+        if (w + 2u < g.NW) t.FLIP[w + 2u] = rr.z;
+        if (w + 3u < g.NW) t.FLIP[w + 3u] = rr.w;
+    }
+}
+
+// Root of tile site x after the open labelling's roots pass: every parent is
+// a run head and every head points at its root.
+__device__ __forceinline__ uint32_t tile_root(const unsigned short *uf, uint32_t x)
+{
+    const uint32_t p = uf[x];
+    const uint32_t q = uf[p];
+    return q == p ? p : q;
+}
+
+// ---------------------------------------------------------------------------
+// Cluster-wide union-find over boundary nodes.
+// ---------------------------------------------------------------------------
+struct Dist {
+    cg::cluster_group cl;
+    uint32_t *HK;
+    unsigned long long *HW;
+    uint32_t hs, hs_log2;
+    int *wrap, *err;
+    uint32_t cap;
+
+    __device__ __forceinline__ unsigned long long *hw(uint32_t node) const
+    {
+        return cl.map_shared_rank(HW, node >> 16) + (node & 0xFFFFu);
+    }
+    __device__ __forceinline__ uint32_t key(uint32_t node) const
+    {
+        return ((node >> 16) << 16) | *((volatile uint32_t *)(cl.map_shared_rank(HK, node >> 16) + (node & 0xFFFFu)));
+    }
+    __device__ __forceinline__ unsigned long long ld(uint32_t node) const
+    {
+        return *((volatile unsigned long long *)hw(node));
+    }
+    __device__ __forceinline__ void st(uint32_t node, unsigned long long v) const
+    {
+        *((volatile unsigned long long *)hw(node)) = v;
+    }
+
+    // Node of tile root `m` in tile `tile` (inserted if new).
+    __device__ __forceinline__ uint32_t insert(uint32_t tile, uint32_t m) const
+    {
+        uint32_t *hk = cl.map_shared_rank(HK, tile);
+        uint32_t h = (m * 0x9E3779B1u) >> (32u - hs_log2);
+        for (uint32_t it = 0; it < hs; ++it) {
+            const uint32_t old = atomicCAS(hk + h, kEmptyKey, m);
+            if (old == kEmptyKey || old == m) return (tile << 16) | h;
+            h = (h + 1u) & (hs - 1u);
+        }
+        atomicOr(err, kErrUnionCap);
+        return (tile << 16) | 0u;
+    }
+
+    __device__ __forceinline__ FindResult find(uint32_t n) const
+    {
+        uint32_t node = n;
+        int ax = 0, ay = 0;
+        unsigned long long w = ld(node);
+        for (uint32_t it = 0;; ++it) {
+            const uint32_t p = Word64::parent(w);
+            if (p == node) break;
+            if (it >= cap) {
+                atomicOr(err, kErrFindCap);
+                break;
+            }
+            const unsigned long long wp = ld(p);
+            const uint32_t gp = Word64::parent(wp);
+            if (gp != p) {
+                const int nx = Word64::ox(w) + Word64::ox(wp), ny = Word64::oy(w) + Word64::oy(wp);
+                st(node, Word64::make(gp, nx, ny));
+                ax += nx;
+                ay += ny;
+                node = gp;
+                w = ld(node);
+            } else {
+                ax += Word64::ox(w);
+                ay += Word64::oy(w);
+                node = p;
+                w = wp;
+            }
+        }
+        return {node, ax, ay};
+    }
+
+    __device__ __forceinline__ uint32_t root_ro(uint32_t n) const
+    {
+        uint32_t node = n;
+        for (uint32_t it = 0;; ++it) {
+            const uint32_t p = Word64::parent(ld(node));
+            if (p == node) break;
+            if (it >= cap) {
+                atomicOr(err, kErrFindCap);
+                break;
+            }
+            node = p;
+        }
+        return node;
+    }
+
+    // Union across a boundary bond a -> b with seam crossing (ex, ey).
+    __device__ __forceinline__ void unite(uint32_t a, uint32_t b, int ex, int ey) const
+    {
+        for (uint32_t it = 0; it < cap; ++it) {
+            const FindResult fa = find(a);
+            const FindResult fb = find(b);
+            if (fa.root == fb.root) {
+                int f = 0;
+                if (Word64::nonzero(ex + fb.ax - fa.ax)) f |= 1;
+                if (Word64::nonzero(ey + fb.ay - fa.ay)) f |= 2;
+                if (f) atomicOr(wrap, f);
+                return;
+            }
+            if (key(fa.root) < key(fb.root)) {
+                const unsigned long long expect = Word64::make(fb.root, 0, 0);
+                const unsigned long long v = Word64::make(fa.root, fa.ax - ex - fb.ax, fa.ay - ey - fb.ay);
+                if (atomicCAS(hw(fb.root), expect, v) == expect) return;
+            } else {
+                const unsigned long long expect = Word64::make(fa.root, 0, 0);
+                const unsigned long long v = Word64::make(fb.root, fb.ax + ex - fa.ax, fb.ay + ey - fa.ay);
+                if (atomicCAS(hw(fa.root), expect, v) == expect) return;
+            }
+        }
+        atomicOr(err, kErrUnionCap);
+    }
+};
+
+// (b) Boundary bonds owned by this tile: x-bonds of its last L sites, the
+// y-bond from its last site into the next tile, and the y-seam bonds of the
+// rows ending in it.
+__device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, const Dist &d, uint32_t tile_end,
+                                              uint32_t tid)
+{
+    const Lat<Word16> &t = x.t;
+    const uint32_t rows_end = (tl.b + tl.Tc) / tl.L;  // rows x0 .. rows_end-1 end in the tile
+    const uint32_t n_rows = rows_end - tl.x0;
+    const uint32_t items = tl.L + 1u + n_rows;
+    const uint32_t nxt = tl.c + 1u == tl.C ? 0u : tl.c + 1u;
+    for (uint32_t i = tid; i < items; i += kCT) {
+        uint32_t a, tb, bl;
+        int ex = 0, ey = 0;
+        if (i < tl.L) {
+            a = tl.Tc - tl.L + i;
+            if (!((t.OH[a >> 5] >> (a & 31u)) & 1u)) continue;
+            const uint32_t n = tl.b + a;
+            if (n + tl.L >= tl.N) {
+                tb = 0u;
+                bl = n + tl.L - tl.N;
+                ex = 1;
+            } else {
+                tb = nxt;
+                bl = a + tl.L - tl.Tc;
+            }
+        } else if (i == tl.L) {
+            if (!tile_end) continue;
+            a = tl.Tc - 1u;
+            tb = nxt;
+            bl = 0u;
+        } else {
+            const uint32_t row = i - tl.L - 1u;
+            if (!((x.YS[row >> 5] >> (row & 31u)) & 1u)) continue;
+            const uint32_t xr = tl.x0 + row;
+            a = xr * tl.L + tl.L - 1u - tl.b;
+            const uint32_t start = xr * tl.L;
+            if (start >= tl.b) {
+                tb = tl.c;
+                bl = start - tl.b;
+            } else {
+                tb = tl.c - 1u;
+                bl = start - (tl.b - tl.T);
+            }
+            ey = 1;
+        }
+        const uint32_t ra = tile_root(t.uf.w, a);
+        const unsigned short *ufb = tb == tl.c ? t.uf.w : d.cl.map_shared_rank(t.uf.w, tb);
+        const uint32_t rb = tile_root(ufb, bl);
+        const uint32_t na = d.insert(tl.c, ra);
+        const uint32_t nb = d.insert(tb, rb);
+        d.unite(na, nb, ex, ey);
+    }
+}
+
+// Spin halo after a flip: the first L spins of the next tile (of the first
+// tile, for the last one) at bits Tc .. Tc+L-1, and the front spin (the row
+// start of the tile's first row, when that row began in the previous tile).
+__device__ __forceinline__ void tile_halo(const Ctx &x, const Tile &tl, const cg::cluster_group &cl, CRed &red,
+                                          uint32_t tid)
+{
+    uint32_t *S = x.t.S;
+    const uint32_t nxt = tl.c + 1u == tl.C ? 0u : tl.c + 1u;
+    const uint32_t *rs = cl.map_shared_rank(S, nxt);
+    const uint32_t lw = (tl.L + 31u) >> 5;
+    const uint32_t sh = tl.Tc & 31u, d0 = tl.Tc >> 5;
+    const uint32_t lmask = (tl.L & 31u) ? (1u << (tl.L & 31u)) - 1u : 0xFFFFFFFFu;
+    for (uint32_t k = tid; k <= lw; k += kCT) {
+        const uint32_t hk = k < lw ? (rs[k] & (k + 1u == lw ? lmask : 0xFFFFFFFFu)) : 0u;
+        uint32_t v;
+        if (sh == 0u) {
+            v = hk;
+        } else {
+            const uint32_t hp = (k > 0u) ? (rs[k - 1u] & (k == lw ? lmask : 0xFFFFFFFFu)) : 0u;
+            v = (hk << sh) | (k > 0u ? hp >> (32u - sh) : 0u);
+            if (k == 0u) v |= S[d0] & ((1u << sh) - 1u);
+        }
+        S[d0 + k] = v;
+    }
+    if (tid == 0) {
+        uint32_t front = 0;
+        if (tl.f) {
+            const uint32_t q = tl.x0 * tl.L - (tl.b - tl.T);
+            const uint32_t *ps = cl.map_shared_rank(S, tl.c - 1u);
+            front = (ps[q >> 5] >> (q & 31u)) & 1u;
+        }
+        red.front = front;
+    }
+}
+
+__device__ __forceinline__ void tile_energy(const Ctx &x, const Tile &tl, const uint32_t *gJH, const uint32_t *gJV,
+                                            uint32_t front, uint32_t tid, uint32_t &unsat, uint32_t &downs)
+{
+    const Lat<Word16> &t = x.t;
+    for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+        const uint32_t v = t.g.valid(w);
+        const uint32_t s = t.S[w];
+        const uint32_t re = tile_row_end(tl, w, v);
+        unsat += __popc((s ^ extract_nowrap(t.S, (w << 5) + tl.L) ^ gJH[w]) & v);
+        unsat += __popc((s ^ tile_ynext(t.S, w, re, tl.L, front) ^ gJV[w]) & v);
+        downs += __popc(s & v);
+    }
+}
+
+// Root node of this tile's node in slot k, once the boundary stage is over
+// (the low word of HW; the high word accumulates merged sizes).
+__device__ __forceinline__ uint32_t node_root(const Ctx &x, uint32_t k)
+{
+    return *((volatile uint32_t *)(x.HW + k));
+}
+
+__device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g)
+{
+    return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
+}
+
+__global__ void __launch_bounds__(kCT, 1)
+    k_cluster_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                     long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *queue, int *status,
+                     ClusterLayout ly)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ CRed red;
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    constexpr uint32_t nwarps = kCT / 32;
+    const uint32_t C = cl.num_blocks(), c = cl.block_rank();
+
+    if (tid == 0) red.err = 0;
+    for (;;) {
+        if (c == 0 && tid == 0) red.item = atomicAdd(queue, 1);
+        cl.sync();
+        if (tid == 0 && c != 0) red.item = *cl.map_shared_rank(&red.item, 0);
+        cl.sync();
+        const int item = red.item;
+        if (item >= n_chains) break;
+        if (tid == 0) {
+            red.ch = chains[item];
+            red.cur_bin = -1;
+        }
+        __syncthreads();
+        const rbim_chain_t &ch = red.ch;
+        const bool bad = ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 ||
+                         ch.n_therm < 0 || !cluster_tiles_ok((uint32_t)ch.L, C) ||
+                         cluster_tile_size((uint32_t)(ch.L * ch.L), C) > ly.t_max;
+        if (bad) {
+            if (tid == 0 && c == 0) atomicOr(status, kErrBadChain);
+            continue;
+        }
+        Tile tl;
+        tl.L = (uint32_t)ch.L;
+        tl.N = tl.L * tl.L;
+        tl.C = C;
+        tl.c = c;
+        tl.T = cluster_tile_size(tl.N, C);
+        tl.b = c * tl.T;
+        tl.Tc = min(tl.T, tl.N - tl.b);
+        tl.tw = (tl.Tc + 31u) >> 5;
+        tl.x0 = tl.b / tl.L;
+        tl.f = tl.b - tl.x0 * tl.L;
+        tl.nwp = (((tl.N + 31u) >> 5) + 3u) & ~3u;
+        const Ctx x = make_ctx(smem, ly, tl, red);
+        const Lat<Word16> &t = x.t;
+        const Dist d{cl, x.HK, x.HW, x.hs, x.hs_log2, &red.wrap, &red.err, C * x.hs + 64u};
+        uint32_t *gS = spin_pool + ch.spin_off + (tl.b >> 5);
+        const uint32_t *gJH = coupling_pool + ch.coupling_off + (tl.b >> 5);
+        const uint32_t *gJV = coupling_pool + ch.coupling_off + tl.nwp + (tl.b >> 5);
+        const uint32_t s_words = ly.tw + (ly.l_max + 31u) / 32u + 4u;
+
+        // Load the tile's spins; zero the halo and padding.
+        for (uint32_t w = tid; w < s_words; w += kCT) t.S[w] = w < tl.tw ? gS[w] & t.g.valid(w) : 0u;
+        const uint64_t t_end = (uint64_t)ch.n_therm + (uint64_t)ch.n_bins * (uint64_t)ch.sweeps_per_bin;
+        uint64_t sweep = ch.sweep;
+        const uint64_t stop = min(t_end, sweep + (uint64_t)max(n_sweeps, 0));
+        cl.sync();
+        tile_halo(x, tl, cl, red, tid);
+        __syncthreads();
+
+        for (; sweep < stop; ++sweep) {
+            const bool measure = sweep >= (uint64_t)ch.n_therm;
+            const uint32_t front = red.front;
+            if (tid == 0) {
+                red.wrap = 0;
+                red.tile_end = 0;
+            }
+            for (uint32_t i = tid; i < 16u; i += kCT) x.YS[i] = 0u;
+            __syncthreads();
+            tile_activate(x, tl, make_rng(ch.key, sweep, ch.thr), gJH, gJV, front, red, warp, nwarps, tid);
+            __syncthreads();
+            phase_heads<Word16>(t, warp, nwarps);
+            for (uint32_t w = tid; w < t.g.NW; w += kCT) t.ROOT[w] = 0u;
+            for (uint32_t k = tid; k < x.hs; k += kCT) {
+                x.HK[k] = kEmptyKey;
+                x.HW[k] = Word64::make((c << 16) | k, 0, 0);
+            }
+            __syncthreads();
+            phase_union_open(t, tid, kCT);
+            __syncthreads();
+            (void)phase_roots_flat(t, tid, kCT);
+            __syncthreads();
+            cl.sync();  // every tile's roots are final
+
+            tile_boundary(x, tl, d, red.tile_end, tid);
+            cl.sync();  // every boundary union is done
+
+            // Root node of each of this tile's nodes, and the flip bit of its
+            // cluster (the raw bit of the root node's site).
+            uint32_t rn[kSlotsPerThread], fb[kSlotsPerThread];
+#pragma unroll
+            for (uint32_t j = 0; j < kSlotsPerThread; ++j) {
+                const uint32_t k = tid + j * kCT;
+                rn[j] = kEmptyKey;
+                fb[j] = 0;
+                if (k < x.hs && x.HK[k] != kEmptyKey) {
+                    const uint32_t r = d.root_ro((c << 16) | k);
+                    rn[j] = r;
+                    const uint32_t m = *cl.map_shared_rank(x.HK + (r & 0xFFFFu), r >> 16);
+                    const uint32_t *fl = cl.map_shared_rank(t.FLIP, r >> 16);
+                    fb[j] = (fl[m >> 5] >> (m & 31u)) & 1u;
+                }
+            }
+            cl.sync();  // all walks done before the words change
+#pragma unroll
+            for (uint32_t j = 0; j < kSlotsPerThread; ++j) {
+                const uint32_t k = tid + j * kCT;
+                if (rn[j] == kEmptyKey) continue;
+                x.HW[k] = (unsigned long long)rn[j];  // root node | merged size (0)
+                if (rn[j] != ((c << 16) | k)) {
+                    const uint32_t m = x.HK[k];
+                    if (fb[j])
+                        atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
+                    else
+                        atomicAnd(t.FLIP + (m >> 5), ~(1u << (m & 31u)));
+                }
+            }
+            __syncthreads();
+            phase_sites<Word16>(t, warp, nwarps, true, false);
+            __syncthreads();
+            cl.sync();  // every flip is done
+            tile_halo(x, tl, cl, red, tid);
+            __syncthreads();
+
+            if (!measure) continue;
+
+            // ---- measurement (reference sw_sweep, src/rbim/swendsen_wang.py:146-172)
+            unsigned short *u16 = t.uf.w;
+            uint32_t unsat = 0, downs = 0;
+            tile_energy(x, tl, gJH, gJV, red.front, tid, unsat, downs);
+            for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+                uint32_t roots = t.ROOT[w];
+                while (roots) {
+                    const uint32_t bb = __ffs(roots) - 1u;
+                    roots &= roots - 1u;
+                    u16[(w << 5) + bb] = 0;
+                }
+            }
+            __syncthreads();
+            // Tile piece sizes minus one into the tile roots' words (a tile
+            // piece may hold all 65536 sites): every run piece adds its
+            // length, the piece that starts at the root one less.
+            for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
+                const uint32_t valid = t.g.valid(w);
+                const uint32_t lead = piece_leaders(t, w, valid);
+                if ((lead >> lane) & 1u) {
+                    const uint32_t n = (w << 5) + lane;
+                    const uint32_t next = lead & ~mask_le(lane);
+                    const uint32_t end = next ? (uint32_t)(__ffs(next) - 1) : (uint32_t)__popc(valid);
+                    const bool is_root = (t.ROOT[w] >> lane) & 1u;
+                    const uint32_t r = is_root ? n : (uint32_t)u16[n];
+                    add16(u16, r, end - lane - (is_root ? 1u : 0u));
+                }
+            }
+            __syncthreads();
+            // OV (no longer needed this sweep) becomes the plane of node marks.
+            for (uint32_t w = tid; w < t.g.NW; w += kCT) t.OV[w] = 0u;
+            __syncthreads();
+            // Merged sizes into the root nodes; mark this tile's nodes in OV.
+            uint32_t rootnodes = 0;
+            for (uint32_t k = tid; k < x.hs; k += kCT) {
+                const uint32_t m = x.HK[k];
+                if (m == kEmptyKey) continue;
+                const uint32_t r = node_root(x, k);
+                atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
+                unsigned int *hi = (unsigned int *)(cl.map_shared_rank(x.HW, r >> 16) + (r & 0xFFFFu)) + 1;
+                atomicAdd(hi, (unsigned int)u16[m] + 1u);
+                if (r == ((c << 16) | k)) ++rootnodes;
+            }
+            __syncthreads();
+            uint32_t nloc = rootnodes;
+            for (uint32_t w = tid; w < t.g.NW; w += kCT) nloc += __popc(t.ROOT[w] & ~t.OV[w]);
+            cl.sync();  // merged sizes are complete
+
+            // Local top two: tile-only clusters and this tile's root nodes.
+            unsigned long long k1 = 0, k2 = 0;
+            for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+                uint32_t roots = t.ROOT[w] & ~t.OV[w];
+                while (roots) {
+                    const uint32_t bb = __ffs(roots) - 1u;
+                    roots &= roots - 1u;
+                    const uint32_t m = (w << 5) + bb;
+                    top2_merge(k1, k2, size_key((uint32_t)u16[m] + 1u, tl.b + m), 0ull);
+                }
+            }
+            for (uint32_t k = tid; k < x.hs; k += kCT) {
+                if (x.HK[k] == kEmptyKey || node_root(x, k) != ((c << 16) | k)) continue;
+                top2_merge(k1, k2, size_key((uint32_t)(x.HW[k] >> 32), tl.b + x.HK[k]), 0ull);
+            }
+            warp_top2(k1, k2);
+            uint32_t u = unsat, dn = downs, nc = nloc;
+            for (int o = 16; o > 0; o >>= 1) {
+                u += __shfl_xor_sync(0xFFFFFFFFu, u, o);
+                dn += __shfl_xor_sync(0xFFFFFFFFu, dn, o);
+                nc += __shfl_xor_sync(0xFFFFFFFFu, nc, o);
+            }
+            if (lane == 0) {
+                red.k1[warp] = k1;
+                red.k2[warp] = k2;
+                red.unsat[warp] = u;
+                red.downs[warp] = dn;
+                red.ncl[warp] = nc;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                unsigned long long a1 = red.k1[lane], a2 = red.k2[lane];
+                warp_top2(a1, a2);
+                uint32_t su = red.unsat[lane], sd = red.downs[lane], sn = red.ncl[lane];
+                for (int o = 16; o > 0; o >>= 1) {
+                    su += __shfl_xor_sync(0xFFFFFFFFu, su, o);
+                    sd += __shfl_xor_sync(0xFFFFFFFFu, sd, o);
+                    sn += __shfl_xor_sync(0xFFFFFFFFu, sn, o);
+                }
+                if (lane == 0) {
+                    red.p_k1 = a1;
+                    red.p_k2 = a2;
+                    red.p_unsat = su;
+                    red.p_downs = sd;
+                    red.p_ncl = sn;
+                    red.p_wrap = red.wrap;
+                }
+            }
+            cl.sync();  // partials are visible
+            long long rec[kRecLen];
+            if (c == 0 && warp == 0) {
+                unsigned long long a1 = 0, a2 = 0;
+                uint32_t su = 0, sd = 0, sn = 0;
+                int wr = 0;
+                if (lane < C) {
+                    const CRed *o = cl.map_shared_rank(&red, lane);
+                    a1 = o->p_k1;
+                    a2 = o->p_k2;
+                    su = o->p_unsat;
+                    sd = o->p_downs;
+                    sn = o->p_ncl;
+                    wr = o->p_wrap;
+                }
+                warp_top2(a1, a2);
+                for (int o = 16; o > 0; o >>= 1) {
+                    su += __shfl_xor_sync(0xFFFFFFFFu, su, o);
+                    sd += __shfl_xor_sync(0xFFFFFFFFu, sd, o);
+                    sn += __shfl_xor_sync(0xFFFFFFFFu, sn, o);
+                    wr |= __shfl_xor_sync(0xFFFFFFFFu, wr, o);
+                }
+                if (lane == 0) {
+                    red.g1 = 0xFFFFFFFFu - (uint32_t)(a1 & 0xFFFFFFFFull);
+                    red.ncl_total = sn;
+                    rec[0] = 2ll * (long long)su - 2ll * (long long)tl.N;
+                    rec[1] = (long long)tl.N - 2ll * (long long)sd;
+                    rec[2] = sn;
+                    rec[3] = (long long)(a1 >> 32);
+                    rec[5] = (long long)(a2 >> 32);
+                    rec[6] = wr & 1;
+                    rec[7] = (wr >> 1) & 1;
+                }
+            }
+            cl.sync();  // rank 0's results are visible
+            if (tid == 0 && c != 0) {
+                const CRed *o = cl.map_shared_rank(&red, 0);
+                red.g1 = o->g1;
+                red.ncl_total = o->ncl_total;
+            }
+            __syncthreads();
+            const uint32_t g1 = red.g1;
+            const bool many = red.ncl_total > 1u;
+            if (many) {
+                // Tile roots of the largest cluster, marked in OH.
+                for (uint32_t w = tid; w < t.g.NW; w += kCT) t.OH[w] = 0u;
+                __syncthreads();
+                if (tid == 0 && g1 >= tl.b && g1 < tl.b + tl.Tc) {
+                    const uint32_t m = g1 - tl.b;
+                    atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
+                }
+                for (uint32_t k = tid; k < x.hs; k += kCT) {
+                    if (x.HK[k] == kEmptyKey) continue;
+                    const uint32_t r = node_root(x, k);
+                    const uint32_t rt = r >> 16;
+                    const uint32_t gr = rt * tl.T + *cl.map_shared_rank(x.HK + (r & 0xFFFFu), rt);
+                    if (gr == g1) {
+                        const uint32_t m = x.HK[k];
+                        atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
+                    }
+                }
+                __syncthreads();
+                int mc = 0;
+                for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
+                    const uint32_t n = (w << 5) + lane;
+                    bool in = false;
+                    if (n < t.g.N) {
+                        const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
+                        in = (t.OH[r >> 5] >> (r & 31u)) & 1u;
+                    }
+                    const uint32_t mm = __ballot_sync(0xFFFFFFFFu, in);
+                    if (lane == 0) mc += (int)__popc(mm) - 2 * (int)__popc(mm & t.S[w]);
+                }
+                if (lane == 0) red.mcw[warp] = mc;
+                __syncthreads();
+                if (tid == 0) {
+                    int s = 0;
+                    for (uint32_t i = 0; i < nwarps; ++i) s += red.mcw[i];
+                    red.p_mc = s;
+                }
+            }
+            cl.sync();  // M_C partials are visible
+            if (c == 0 && tid == 0) {
+                long long mc_total = rec[1];
+                if (many) {
+                    mc_total = 0;
+                    for (uint32_t i = 0; i < C; ++i) mc_total += cl.map_shared_rank(&red, i)->p_mc;
+                }
+                rec[4] = mc_total < 0 ? -mc_total : mc_total;
+                const long long idx = (long long)(sweep - (uint64_t)ch.n_therm);
+                const long long bin = idx / ch.sweeps_per_bin;
+                if (bin != red.cur_bin) {
+                    if (red.cur_bin >= 0)
+                        red.acc.store(acc_i + (ch.acc_off + red.cur_bin) * kAccInt,
+                                      acc_f + (ch.acc_off + red.cur_bin) * kAccF64);
+                    red.acc.load(acc_i + (ch.acc_off + bin) * kAccInt, acc_f + (ch.acc_off + bin) * kAccF64);
+                    red.cur_bin = bin;
+                }
+                red.acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[6], (int)rec[7]);
+                if (records && ch.rec_off >= 0) {
+                    int32_t *row = records + (ch.rec_off + idx) * kRecLen;
+#pragma unroll
+                    for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];
+                }
+            }
+        }
+        if (c == 0 && tid == 0) {
+            if (red.cur_bin >= 0)
+                red.acc.store(acc_i + (ch.acc_off + red.cur_bin) * kAccInt,
+                              acc_f + (ch.acc_off + red.cur_bin) * kAccF64);
+            chains[item].sweep = stop;
+        }
+        for (uint32_t w = tid; w < tl.tw; w += kCT) gS[w] = t.S[w] & t.g.valid(w);
+        cl.sync();  // halo reads of this chain are over before the next load
+    }
+    if (tid == 0 && red.err) atomicOr(status, red.err);
+}
+
+}  // namespace
+
+cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters)
+{
+    *clusters = 0;
+    const ClusterLayout ly = cluster_layout(l_max, C);
+    if (!cluster_layout_fits(ly)) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_cluster_sweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ly.bytes);
+    if (e != cudaSuccess) return e;
+    if (C > 8u) {
+        e = cudaFuncSetAttribute(k_cluster_sweeps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(kCT, 1, 1);
+    cfg.dynamicSmemBytes = ly.bytes;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(clusters, k_cluster_sweeps, &cfg);
+}
+
+cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
+                                  const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
+                                  int n_sweeps, int *queue, int *status, cudaStream_t stream)
+{
+    const uint32_t C = cluster_size_for((uint32_t)l_max);
+    if (C == 0) return cudaErrorInvalidValue;
+    int clusters = 0;
+    cudaError_t e = cluster_occupancy((uint32_t)l_max, C, &clusters);
+    if (e != cudaSuccess) return e;
+    if (clusters <= 0) return cudaErrorInvalidConfiguration;
+    const ClusterLayout ly = cluster_layout((uint32_t)l_max, C);
+    const int n_clusters = std::min(clusters, n_chains);
+    e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)n_clusters * C, 1, 1);
+    cfg.blockDim = dim3(kCT, 1, 1);
+    cfg.dynamicSmemBytes = ly.bytes;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_cluster_sweeps, const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
+                           coupling_pool, acc_i, acc_f, rec, n_sweeps, queue, status, ly);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+}  // namespace rbim

@@ -38,4 +38,36 @@ cudaError_t launch_plain_label(int64_t L, const uint8_t *occ, int32_t *labels, i
 int resident_max_l();
 int resident_default_threads(int l_max);
 
+// Cluster engine (one lattice per thread-block cluster of C CTAs, one tile of
+// at most 65536 consecutive sites per CTA).
+struct ClusterLayout {
+    uint32_t l_max, C, t_max, tw, hs;
+    size_t off_uf, off_S, off_OH, off_OV, off_FLIP, off_ROOT, off_YS, off_HK, off_HW, bytes;
+};
+
+// Tile size of an N-site lattice split over C CTAs: ceil(N / C) rounded up to
+// a multiple of 128 sites, so that tiles start on Philox chunk boundaries.
+__host__ __device__ inline uint32_t cluster_tile_size(uint32_t N, uint32_t C)
+{
+    const uint32_t t = (N + C - 1u) / C;
+    return (t + 127u) & ~127u;
+}
+
+// C tiles fit an L x L lattice when every tile holds between L and 65536 sites.
+__host__ __device__ inline bool cluster_tiles_ok(uint32_t L, uint32_t C)
+{
+    const uint32_t N = L * L, T = cluster_tile_size(N, C);
+    if (T > 65536u || T < L) return false;
+    const uint32_t before = (C - 1u) * T;
+    return before < N && N - before >= L;
+}
+
+uint32_t cluster_size_for(uint32_t L);
+ClusterLayout cluster_layout(uint32_t l_max, uint32_t C);
+bool cluster_layout_fits(const ClusterLayout &ly);
+cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters);
+cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
+                                  const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
+                                  int n_sweeps, int *queue, int *status, cudaStream_t stream);
+
 }  // namespace rbim

@@ -138,6 +138,21 @@ class ChainSet:
         self.records = torch.zeros((tr, _native.REC_LEN), dtype=torch.int32, device=self.device) if tr else None
         self.spin_off, self.acc_off, self.rec_off = s_off, a_off, r_off
 
+        # Descriptor slots: chains for the resident engine first, then those for
+        # the cluster engine, then those only the plain engine takes.
+        with torch.cuda.device(self.device):
+            r_max = _native.resident_max_l()
+            c_max = _native.cluster_max_l()
+        cls = np.where(Ls <= r_max, 0, np.where(Ls <= c_max, 1, 2))
+        order = np.argsort(cls, kind="stable")
+        self.slot = np.empty(self.n, dtype=np.int64)
+        self.slot[order] = np.arange(self.n)
+        self.n_resident = int(np.sum(cls == 0))
+        self.n_cluster = int(np.sum(cls == 1))
+        self.l_max_resident = int(Ls[cls == 0].max()) if self.n_resident else 0
+        self.l_max_cluster = int(Ls[cls == 1].max()) if self.n_cluster else 0
+        self.plain_only = [int(i) for i in order[self.n_resident + self.n_cluster:]]
+
         desc = np.zeros(self.n, dtype=_native.CHAIN_DTYPE)
         desc["key"] = [s.key for s in self.specs]
         desc["thr"] = [threshold(s.beta) for s in self.specs]
@@ -149,6 +164,7 @@ class ChainSet:
         desc["n_bins"] = [s.n_bins for s in self.specs]
         desc["sweeps_per_bin"] = [s.sweeps_per_bin for s in self.specs]
         desc["L"] = Ls
+        desc = desc[order]
         self.desc_host = desc
         self.chains = torch.from_numpy(desc.view(np.uint8).copy()).to(self.device)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -185,9 +201,10 @@ class ChainSet:
 
     def set_sweep(self, i: int, sweep: int) -> None:
         """Set chain ``i``'s sweep counter (host and device copies)."""
-        self.desc_host["sweep"][i] = sweep
-        row = _torch().from_numpy(self.desc_host[i: i + 1].view(np.uint8).copy())
-        self.chains[96 * i: 96 * (i + 1)].copy_(row)
+        k = int(self.slot[i])
+        self.desc_host["sweep"][k] = sweep
+        row = _torch().from_numpy(self.desc_host[k: k + 1].view(np.uint8).copy())
+        self.chains[96 * k: 96 * (k + 1)].copy_(row)
         self._sweep_host[i] = min(sweep, self.n_total[i])
 
     def spin_words(self, i: int) -> np.ndarray:
@@ -199,19 +216,40 @@ class ChainSet:
 
     # -- sweeps ------------------------------------------------------------
     def run_batched(self, n_sweeps: int, threads: int = 0) -> None:
-        """Advance every chain by up to ``n_sweeps`` sweeps on the resident engine (one launch)."""
+        """Advance every chain by up to ``n_sweeps`` sweeps.
+
+        Chains with L up to ``rbim_resident_max_l()`` run in one launch of the
+        resident engine (one lattice per CTA), larger ones up to
+        ``rbim_cluster_max_l()`` in one launch of the cluster engine (one
+        lattice per thread-block cluster), and any larger still on the plain
+        engine.
+        """
         if n_sweeps <= 0:
             return
         nbytes = int(self.lib.rbim_batched_workspace_bytes())
         ws = self._workspace(nbytes)
+        recs = self._ptr(self.records) if self.records is not None else None
         with _torch().cuda.device(self.device):
-            rc = self.lib.rbim_sweeps_batched(
-                self._ptr(self.chains), self.n, self.l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
-                self._ptr(self.acc_int), self._ptr(self.acc_f64),
-                self._ptr(self.records) if self.records is not None else None,
-                int(n_sweeps), int(threads), self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
-        _native.check(rc, "rbim_sweeps_batched")
-        self._sweep_host = np.minimum(self._sweep_host + n_sweeps, self.n_total)
+            if self.n_resident:
+                rc = self.lib.rbim_sweeps_batched(
+                    self._ptr(self.chains), self.n_resident, self.l_max_resident, self._ptr(self.spin_pool),
+                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64), recs,
+                    int(n_sweeps), int(threads), self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
+                _native.check(rc, "rbim_sweeps_batched")
+            if self.n_cluster:
+                rc = self.lib.rbim_sweeps_clustered(
+                    ctypes.c_void_p(self.chains.data_ptr() + 96 * self.n_resident), self.n_cluster,
+                    self.l_max_cluster, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
+                    self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), self._ptr(self.status),
+                    self._ptr(ws), ws.numel(), self._stream())
+                _native.check(rc, "rbim_sweeps_clustered")
+        if self.plain_only:
+            self.run_plain(n_sweeps, self.plain_only)
+            done = np.ones(self.n, dtype=bool)
+            done[self.plain_only] = False
+            self._sweep_host[done] = np.minimum(self._sweep_host[done] + n_sweeps, self.n_total[done])
+        else:
+            self._sweep_host = np.minimum(self._sweep_host + n_sweeps, self.n_total)
 
     def run_plain(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> None:
         """Advance chains one at a time on the plain (global-memory) engine."""
@@ -223,7 +261,7 @@ class ChainSet:
         with _torch().cuda.device(self.device):
             for i in idx:
                 rc = self.lib.rbim_sweeps_plain(
-                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * i), self._ptr(self.spin_pool),
+                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * int(self.slot[i])), self._ptr(self.spin_pool),
                     self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
                     self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
                     self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
@@ -242,7 +280,7 @@ class ChainSet:
         with _torch().cuda.device(self.device):
             for i in idx:
                 rc = self.lib.rbim_sweeps_plain_noalloc(
-                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * i), self._ptr(self.spin_pool),
+                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * int(self.slot[i])), self._ptr(self.spin_pool),
                     self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
                     self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
                     self._ptr(self.status), self._stream())
@@ -256,7 +294,7 @@ class ChainSet:
     def run_to_end(self, engine: str = "auto", chunk: int = 1000, threads: int = 0) -> None:
         """Run every chain to the end of its run in chunks of ``chunk`` sweeps."""
         if engine == "auto":
-            engine = "batched" if self.l_max <= _native.resident_max_l() else "plain"
+            engine = "batched"
         if engine not in ("batched", "plain"):
             raise ValueError(f"engine must be 'auto', 'batched' or 'plain', got {engine!r}")
         while self.remaining() > 0:
@@ -276,7 +314,7 @@ class ChainSet:
     def device_sweeps(self) -> np.ndarray:
         """The chains' sweep counters as stored on the device."""
         d = self.chains.cpu().numpy().view(_native.CHAIN_DTYPE)
-        return d["sweep"].astype(np.int64)
+        return d["sweep"].astype(np.int64)[self.slot]
 
     def bins(self, i: int):
         """``(int_sums (n_bins, 12), f64_sums (n_bins, 2))`` of chain ``i`` (host copies)."""

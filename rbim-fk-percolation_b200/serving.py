@@ -16,8 +16,9 @@ into launches, so every result equals the one ``run_temperature_scan`` gives
 for the same request alone, bit for bit.
 
 Lattices with L up to ``rbim_resident_max_l()`` run on the resident engine,
-one lattice per CTA; larger ones run on the plain engine, one chain after the
-other inside each quantum.
+one lattice per CTA; larger ones up to ``rbim_cluster_max_l()`` on the
+cluster engine, one lattice per thread-block cluster; any larger still on the
+plain engine, one chain after the other inside each quantum.
 """
 
 from __future__ import annotations
@@ -162,7 +163,9 @@ class ScanServer:
         self.quantum = int(quantum)
         self.threads = int(threads)
         self.max_chains = int(max_chains)
-        self.resident_max_l = _native.resident_max_l()
+        with torch.cuda.device(self.device):
+            self.resident_max_l = _native.resident_max_l()
+            self.cluster_max_l = _native.cluster_max_l()
         words = int(memory_bytes * 0.75) // 4
         rows = int(memory_bytes * 0.25) // 112
         self.words = RangeAllocator(words, align=4)
@@ -328,9 +331,11 @@ class ScanServer:
         sp = ctypes.c_void_p(self.stream.cuda_stream)
         pool = ctypes.c_void_p(self.word_pool.data_ptr())
         ai, af = ctypes.c_void_p(self.acc_int.data_ptr()), ctypes.c_void_p(self.acc_f64.data_ptr())
-        resident = [a for a in self._active if a.plan.L <= self.resident_max_l and a.done < a.n_total]
-        plain = [a for a in self._active if a.plan.L > self.resident_max_l and a.done < a.n_total]
-        descs = [a.desc for a in resident] + [a.desc for a in plain]
+        live = [a for a in self._active if a.done < a.n_total]
+        resident = [a for a in live if a.plan.L <= self.resident_max_l]
+        clustered = [a for a in live if self.resident_max_l < a.plan.L <= self.cluster_max_l]
+        plain = [a for a in live if a.plan.L > max(self.resident_max_l, self.cluster_max_l)]
+        descs = [a.desc for a in resident] + [a.desc for a in clustered] + [a.desc for a in plain]
         if not descs:
             return
         allc = np.concatenate(descs)
@@ -351,12 +356,22 @@ class ScanServer:
                                                   ctypes.c_void_p(self.queue_ws.data_ptr()), self.queue_ws.numel(), sp)
                 _native.check(rc, "rbim_sweeps_batched")
                 self.launches += 1
+            n_clu = sum(len(a.desc) for a in clustered)
+            if n_clu:
+                l_max = max(a.plan.L for a in clustered)
+                rc = self.lib.rbim_sweeps_clustered(ctypes.c_void_p(self.desc_dev.data_ptr() + 96 * n_res), n_clu,
+                                                    l_max, pool, pool, ai, af, None, self.quantum,
+                                                    ctypes.c_void_p(self.status.data_ptr()),
+                                                    ctypes.c_void_p(self.queue_ws.data_ptr()), self.queue_ws.numel(),
+                                                    sp)
+                _native.check(rc, "rbim_sweeps_clustered")
+                self.launches += 1
             if plain:
                 l_big = max(a.plan.L for a in plain)
                 need = int(self.lib.rbim_plain_workspace_bytes(l_big))
                 if self._plain_ws is None or self._plain_ws.numel() < need:
                     self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
-                base = self.desc_dev.data_ptr() + 96 * n_res
+                base = self.desc_dev.data_ptr() + 96 * (n_res + n_clu)
                 k = 0
                 for a in plain:
                     for _ in range(len(a.desc)):
@@ -367,7 +382,7 @@ class ScanServer:
                         _native.check(rc, "rbim_sweeps_plain")
                         self.launches += 1
                         k += 1
-        for a in resident + plain:
+        for a in live:
             a.done = min(a.n_total, a.done + self.quantum)
             a.desc["sweep"] = a.done
 
