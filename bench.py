@@ -177,6 +177,120 @@ def cpu_baseline(L, temps, ps, seconds=10.0, threads=0):
             "sample": f"{n_threads} chains of L={L} x {sweeps} measured sweeps, one chain per thread ({dt:.1f} s)"}
 
 
+def time_sweeps(cs, n, plain=False):
+    """Device time of n sweeps of every chain of a ChainSet (CUDA events on the current stream)."""
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    if plain:
+        cs.run_plain(n)
+    else:
+        cs.run_batched(n)
+    e1.record()
+    e1.synchronize()
+    cs.check_status()
+    return e0.elapsed_time(e1) / 1000.0
+
+
+def config_lines(rb, dev, seed):
+    """Throughput of the other configurations: batched vs plain at L = 64 (256 realizations x 64 T),
+    the L = 512 slice of the uneven-size mix and L = 1024 (cluster engine), one L = 1024 lattice."""
+    out = {}
+
+    def chainset(L, p, n_real, temps, n_total, s):
+        specs, couplings = build_chains(rb, L, [p], n_real, temps, s, n_total)
+        cs = rb.ChainSet(specs, couplings, device=dev)
+        cs.init_spins(hot=True)
+        return cs, specs, couplings
+
+    # Batched, uniform size: L = 64, p = 0.05, 256 x 64 chains.
+    cs, specs, couplings = chainset(64, 0.05, 256, np.linspace(1.0, 3.0, 64), 1000, seed)
+    cs.run_batched(3)
+    t = time_sweeps(cs, 10)
+    b = len(specs) * 10 / t
+    pcs = rb.ChainSet(specs[:1], couplings[:1], device=dev)
+    pcs.init_spins(hot=True)
+    pcs.run_plain(5)
+    pt = time_sweeps(pcs, 200, plain=True)
+    pv = 200 / pt
+    out["c3_L64"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 4096,
+                     "plain_lattice_sweeps_per_s": pv, "plain_site_updates_per_s": pv * 4096,
+                     "batched_over_plain": b / pv, "chains": len(specs), "engine": "resident"}
+    del cs, pcs
+    # The L = 512 slice of the uneven-size mix: 16 realizations x 4 p x 32 T.
+    specs, couplings = build_chains(rb, 512, [0.02, 0.05, 0.08, 0.10], 16, np.linspace(1.2, 2.4, 32), seed, 1000)
+    cs = rb.ChainSet(specs, couplings, device=dev)
+    cs.init_spins(hot=True)
+    cs.run_batched(1)
+    t = time_sweeps(cs, 3)
+    b = len(specs) * 3 / t
+    pcs = rb.ChainSet(specs[:1], couplings[:1], device=dev)
+    pcs.init_spins(hot=True)
+    pcs.run_plain(3)
+    pv = 50 / time_sweeps(pcs, 50, plain=True)
+    out["c4_L512"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 512 * 512,
+                      "plain_lattice_sweeps_per_s": pv, "batched_over_plain": b / pv, "chains": len(specs),
+                      "engine": "cluster (4 CTAs per lattice)"}
+    del cs, pcs
+    # L = 1024: one lattice (p = 0.10, T = 1.6) on the plain and the cluster engine, and 128 lattices batched.
+    cs, specs, couplings = chainset(1024, 0.10, 4, np.linspace(1.5, 1.7, 32), 1000, seed)
+    cs.run_batched(1)
+    t = time_sweeps(cs, 3)
+    b = len(specs) * 3 / t
+    one = rb.ChainSet([rb.ChainSpec(L=1024, realization=0, key=specs[0].key, beta=1 / 1.6, n_therm=0, n_bins=1,
+                                    sweeps_per_bin=1000)], couplings[:1], device=dev)
+    one.init_spins(hot=True)
+    one.run_batched(2)
+    ov = 20 / time_sweeps(one, 20)
+    one.run_plain(2)
+    pv = 20 / time_sweeps(one, 20, plain=True)
+    out["c2_L1024"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 1024 * 1024,
+                       "one_lattice_cluster_sweeps_per_s": ov, "one_lattice_plain_sweeps_per_s": pv,
+                       "batched_over_plain": b / pv, "chains": len(specs), "engine": "cluster (16 CTAs per lattice)"}
+    return out
+
+
+def serving_leg(rb, dev, seconds, rate, scale, seed, quantum):
+    """Poisson stream of temperature-scan requests (the serving configuration's distribution of L, p,
+    temperatures and realizations, sweeps scaled by `scale`) through the continuous-batching server."""
+    rng = np.random.default_rng(seed)
+    arrivals, reqs, work = [], [], 0
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        L = int(rng.choice([16, 32, 64, 128, 256, 512]))
+        n_t = int(rng.integers(8, 65))
+        n_r = int(rng.integers(4, 65))
+        sweeps = max(10, int(round(int(rng.integers(1000, 10001)) * scale)))
+        req = rb.ScanRequest(L=L, p=float(rng.uniform(0.0, 0.12)), temperatures=np.linspace(1.0, 3.0, n_t),
+                             n_realizations=n_r, n_sweeps=sweeps, n_bins=10, seed=int(rng.integers(2**31)))
+        arrivals.append(t)
+        reqs.append(req)
+        work += n_t * n_r * (sweeps + max(1, sweeps // 10)) * L * L
+    server = rb.ScanServer(device=dev, memory_bytes=8 << 30, quantum=quantum)
+    with server:
+        t0 = time.perf_counter()
+        futs = []
+        for at, req in zip(arrivals, reqs):
+            now = time.perf_counter() - t0
+            if at > now:
+                time.sleep(at - now)
+            futs.append(server.submit(req))
+        for f in futs:
+            f.result()
+        t_end = time.perf_counter() - t0
+    pct = server.latency_percentiles((50, 99))
+    served = sum(c["site_updates"] for c in server.completed)
+    return {"p50_s": pct["p50"], "p99_s": pct["p99"], "requests": len(reqs), "arrival_window_s": seconds,
+            "rate_per_s": rate, "sweep_scale": scale, "quantum_sweeps": quantum, "wall_s": t_end,
+            "offered_site_updates_per_s": work / seconds, "served_site_updates_per_s": served / t_end,
+            "launches": server.launches}
+
+
 def run_reference(args, L, ps, temps, metric):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -217,6 +331,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--chains", type=int, default=0, help="use only the first N chains (profiling runs)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' lines")
+    ap.add_argument("--serve-seconds", type=float, default=12.0, help="serving leg arrival window (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-scale", type=float, default=0.004, help="sweeps per request scaled by this factor")
+    ap.add_argument("--serve-quantum", type=int, default=10)
     args = ap.parse_args()
 
     L, ps, n_real, temps = workload(args.workload)
@@ -342,6 +461,14 @@ def main():
                "d2h_bytes_per_step": int(d2h), "api": "run_temperature_scan (4 calls per step)",
                "sweeps_per_chain": E + E // 10}
 
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = config_lines(rb, dev, args.seed)
+    serving = None
+    if rank == 0 and args.serve_seconds > 0:
+        serving = serving_leg(rb, dev, args.serve_seconds, args.serve_rate, args.serve_scale, args.seed,
+                              args.serve_quantum)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(L, temps, ps, seconds=args.cpu_seconds)
@@ -376,6 +503,8 @@ def main():
         "gpu_launches": args.steps,
         "e2e": e2e,
         "plain": plain,
+        "serving": serving,
+        "configs": configs,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

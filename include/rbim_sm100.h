@@ -173,6 +173,8 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
  * be scheduled).
  */
 int rbim_cluster_max_l(void);
+/* CTAs per cluster the cluster engine uses for an L x L lattice (0 if none). */
+int rbim_cluster_size(int64_t L);
 int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
                           const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
                           int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream);

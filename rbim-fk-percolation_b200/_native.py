@@ -25,6 +25,7 @@ __all__ = [
     "plane_words",
     "resident_max_l",
     "cluster_max_l",
+    "engine_buckets",
     "EXPORTED_SYMBOLS",
 ]
 
@@ -67,6 +68,7 @@ EXPORTED_SYMBOLS = (
     "rbim_plain_workspace_bytes",
     "rbim_sweeps_plain",
     "rbim_cluster_max_l",
+    "rbim_cluster_size",
     "rbim_sweeps_clustered",
     "rbim_noalloc_max_l",
     "rbim_sweeps_plain_noalloc",
@@ -111,6 +113,8 @@ def _declare(l):
     l.rbim_sweeps_plain.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p, c_size, p]
     l.rbim_cluster_max_l.restype = c_int
     l.rbim_cluster_max_l.argtypes = []
+    l.rbim_cluster_size.restype = c_int
+    l.rbim_cluster_size.argtypes = [c_i64]
     l.rbim_sweeps_clustered.restype = c_int
     l.rbim_sweeps_clustered.argtypes = [p, c_int, c_i64, p, p, p, p, p, c_int, p, p, c_size, p]
     l.rbim_noalloc_max_l.restype = c_int
@@ -159,6 +163,25 @@ def plane_words(L: int) -> int:
 def resident_max_l() -> int:
     """Largest L the on-chip engine takes (``rbim_resident_max_l``)."""
     return int(lib().rbim_resident_max_l())
+
+
+def engine_buckets(Ls, r_max: int, c_max: int):
+    """Launch bucket of every lattice size: ``(kind, key)`` with kind 0 resident, 1 cluster, 2 plain.
+
+    Resident lattices are bucketed by power-of-two size class (the resident
+    launch sizes its CTAs for the bucket's largest L), cluster lattices by
+    CTAs per cluster; buckets sort in launch order.
+    """
+    out = []
+    for L in Ls:
+        L = int(L)
+        if L <= r_max:
+            out.append((0, max(4, (L - 1).bit_length())))
+        elif L <= c_max:
+            out.append((1, int(lib().rbim_cluster_size(L))))
+        else:
+            out.append((2, 0))
+    return out
 
 
 def cluster_max_l() -> int:

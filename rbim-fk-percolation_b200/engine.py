@@ -138,20 +138,22 @@ class ChainSet:
         self.records = torch.zeros((tr, _native.REC_LEN), dtype=torch.int32, device=self.device) if tr else None
         self.spin_off, self.acc_off, self.rec_off = s_off, a_off, r_off
 
-        # Descriptor slots: chains for the resident engine first, then those for
-        # the cluster engine, then those only the plain engine takes.
+        # Descriptor slots grouped by launch bucket: resident lattices by size
+        # class, cluster lattices by CTAs per cluster, then those only the plain
+        # engine takes (engine_buckets).
         with torch.cuda.device(self.device):
             r_max = _native.resident_max_l()
             c_max = _native.cluster_max_l()
-        cls = np.where(Ls <= r_max, 0, np.where(Ls <= c_max, 1, 2))
-        order = np.argsort(cls, kind="stable")
+            keys = _native.engine_buckets(Ls, r_max, c_max)
+        order = np.array(sorted(range(self.n), key=lambda i: keys[i]), dtype=np.int64)
         self.slot = np.empty(self.n, dtype=np.int64)
         self.slot[order] = np.arange(self.n)
-        self.n_resident = int(np.sum(cls == 0))
-        self.n_cluster = int(np.sum(cls == 1))
-        self.l_max_resident = int(Ls[cls == 0].max()) if self.n_resident else 0
-        self.l_max_cluster = int(Ls[cls == 1].max()) if self.n_cluster else 0
-        self.plain_only = [int(i) for i in order[self.n_resident + self.n_cluster:]]
+        self.buckets = []  # (kind, first slot, count, l_max)
+        for k in sorted(set(keys)):
+            members = [i for i in range(self.n) if keys[i] == k]
+            first = int(min(self.slot[i] for i in members))
+            self.buckets.append((k[0], first, len(members), int(max(Ls[i] for i in members))))
+        self.plain_only = [int(i) for i in order if keys[i][0] == 2]
 
         desc = np.zeros(self.n, dtype=_native.CHAIN_DTYPE)
         desc["key"] = [s.key for s in self.specs]
@@ -218,11 +220,11 @@ class ChainSet:
     def run_batched(self, n_sweeps: int, threads: int = 0) -> None:
         """Advance every chain by up to ``n_sweeps`` sweeps.
 
-        Chains with L up to ``rbim_resident_max_l()`` run in one launch of the
-        resident engine (one lattice per CTA), larger ones up to
-        ``rbim_cluster_max_l()`` in one launch of the cluster engine (one
-        lattice per thread-block cluster), and any larger still on the plain
-        engine.
+        Chains with L up to ``rbim_resident_max_l()`` run on the resident
+        engine (one lattice per CTA, one launch per power-of-two size class),
+        larger ones up to ``rbim_cluster_max_l()`` on the cluster engine (one
+        lattice per thread-block cluster, one launch per cluster size), and
+        any larger still on the plain engine.
         """
         if n_sweeps <= 0:
             return
@@ -230,19 +232,20 @@ class ChainSet:
         ws = self._workspace(nbytes)
         recs = self._ptr(self.records) if self.records is not None else None
         with _torch().cuda.device(self.device):
-            if self.n_resident:
-                rc = self.lib.rbim_sweeps_batched(
-                    self._ptr(self.chains), self.n_resident, self.l_max_resident, self._ptr(self.spin_pool),
-                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64), recs,
-                    int(n_sweeps), int(threads), self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
-                _native.check(rc, "rbim_sweeps_batched")
-            if self.n_cluster:
-                rc = self.lib.rbim_sweeps_clustered(
-                    ctypes.c_void_p(self.chains.data_ptr() + 96 * self.n_resident), self.n_cluster,
-                    self.l_max_cluster, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
-                    self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), self._ptr(self.status),
-                    self._ptr(ws), ws.numel(), self._stream())
-                _native.check(rc, "rbim_sweeps_clustered")
+            for kind, first, count, l_max in self.buckets:
+                ptr = ctypes.c_void_p(self.chains.data_ptr() + 96 * first)
+                if kind == 0:
+                    rc = self.lib.rbim_sweeps_batched(
+                        ptr, count, l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
+                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), int(threads),
+                        self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
+                    _native.check(rc, "rbim_sweeps_batched")
+                elif kind == 1:
+                    rc = self.lib.rbim_sweeps_clustered(
+                        ptr, count, l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
+                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps),
+                        self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
+                    _native.check(rc, "rbim_sweeps_clustered")
         if self.plain_only:
             self.run_plain(n_sweeps, self.plain_only)
             done = np.ones(self.n, dtype=bool)

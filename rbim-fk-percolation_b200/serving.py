@@ -27,8 +27,8 @@ import ctypes
 import queue
 import threading
 import time
-from concurrent.futures import Future
-from dataclasses import dataclass, field
+from concurrent.futures import Future, ThreadPoolExecutor
+from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -109,6 +109,12 @@ class RangeAllocator:
         return max((s for _, s in self.free), default=0)
 
 
+def _plan_and_pack(req: ScanRequest):
+    plan = req.plan()
+    packed = [pack_couplings(J, plan.L) for J in plan.couplings]
+    return plan, (np.concatenate(packed).view(np.int32) if packed else np.zeros(0, np.int32))
+
+
 def request_footprint(L: int, n_temperatures: int, n_realizations: int, n_bins: int) -> Dict[str, int]:
     """Device footprint of a request: pool words (spins + couplings), accumulator rows, chains.
 
@@ -135,6 +141,7 @@ class _Active:
     desc: np.ndarray  # CHAIN_DTYPE, one per chain, sweep tracked on the host
     n_total: int
     done: int = 0
+    staged: object = None  # host and device staging of the admission copies
 
 
 @dataclass
@@ -142,8 +149,7 @@ class _Pending:
     req: ScanRequest
     future: Future
     submitted: float
-    plan: Optional[ScanPlan] = None
-    meta: dict = field(default_factory=dict)
+    planned: Optional[Future] = None  # -> (ScanPlan, packed couplings)
 
 
 class ScanServer:
@@ -172,6 +178,7 @@ class ScanServer:
         self.rows = RangeAllocator(rows, align=1)
         with torch.cuda.device(self.device):
             self.stream = torch.cuda.Stream(self.device)
+            self.copy_stream = torch.cuda.Stream(self.device)
             self.word_pool = torch.zeros(max(self.words.capacity, 4), dtype=torch.int32, device=self.device)
             self.acc_int = torch.zeros((max(self.rows.capacity, 1), _native.ACC_INT), dtype=torch.int64,
                                        device=self.device)
@@ -184,9 +191,11 @@ class ScanServer:
             self.queue_ws = torch.zeros(int(self.lib.rbim_batched_workspace_bytes()), dtype=torch.uint8,
                                         device=self.device)
         self._plain_ws = None
+        self._planner = ThreadPoolExecutor(max_workers=2, thread_name_prefix="rbim-scan-plan")
         self._inbox: "queue.Queue[_Pending]" = queue.Queue()
         self._waiting: List[_Pending] = []
         self._active: List[_Active] = []
+        self._inflight: list = []  # (event after a launch, requests that launch finished)
         self._thread = None
         self._stop = threading.Event()
         self._error: Optional[BaseException] = None
@@ -203,7 +212,11 @@ class ScanServer:
             raise ValueError(f"request needs {fp} which exceeds the server's pools "
                              f"(words {self.words.capacity}, rows {self.rows.capacity}, chains {self.max_chains})")
         fut: Future = Future()
-        self._inbox.put(_Pending(request, fut, time.perf_counter()))
+        p = _Pending(request, fut, time.perf_counter())
+        # Disorder, keys and packed couplings are prepared on the host while
+        # earlier requests run.
+        p.planned = self._planner.submit(_plan_and_pack, request)
+        self._inbox.put(p)
         return fut
 
     def __enter__(self):
@@ -223,9 +236,10 @@ class ScanServer:
         self._stop.set()
         self._thread.join()
         self._thread = None
+        self._planner.shutdown(wait=False)
 
     def idle(self) -> bool:
-        return not self._active and not self._waiting and self._inbox.empty()
+        return not self._active and not self._waiting and not self._inflight and self._inbox.empty()
 
     # -- server side --------------------------------------------------------
     def _loop(self) -> None:
@@ -271,9 +285,15 @@ class ScanServer:
         n_chains = sum(len(a.desc) for a in self._active)
         while self._waiting:
             p = self._waiting[0]
-            if p.plan is None:
-                p.plan = p.req.plan()
-            plan = p.plan
+            if not p.planned.done() and self._active:
+                return  # keep the device busy; admit once the plan is ready
+            try:
+                plan, packed = p.planned.result()
+            except BaseException as exc:  # a bad request fails alone
+                self._waiting.pop(0)
+                p.future.set_exception(exc)
+                self._inbox.task_done()
+                continue
             nw = words_for(plan.L)
             n_r = plan.n_realizations
             chains = plan.n_tasks
@@ -297,7 +317,6 @@ class ScanServer:
             spin_off = w_off
             coup_off = w_off + chains * nw
             # Couplings and zeroed accumulators, then the hot or cold start.
-            packed = np.concatenate([pack_couplings(J, plan.L) for J in plan.couplings]).view(np.int32)
             desc = np.zeros(chains, dtype=_native.CHAIN_DTYPE)
             t_index = np.arange(chains) // n_r
             real = np.arange(chains) % n_r
@@ -311,18 +330,22 @@ class ScanServer:
             desc["n_bins"] = plan.n_bins
             desc["sweeps_per_bin"] = plan.sweeps_per_bin
             desc["L"] = plan.L
+            # Pinned staging keeps the copies asynchronous behind the running
+            # launch; the staging tensors live until the request retires.
+            staged = (torch.from_numpy(packed).pin_memory(), torch.from_numpy(desc.view(np.uint8).copy()).pin_memory())
             with torch.cuda.stream(self.stream):
-                self.word_pool[coup_off: coup_off + packed.size].copy_(torch.from_numpy(packed), non_blocking=False)
+                self.word_pool[coup_off: coup_off + packed.size].copy_(staged[0], non_blocking=True)
                 self.acc_int[r_off: r_off + chains * plan.n_bins].zero_()
                 self.acc_f64[r_off: r_off + chains * plan.n_bins].zero_()
-                d = torch.from_numpy(desc.view(np.uint8).copy()).to(self.device)
+                d = torch.empty(staged[1].numel(), dtype=torch.uint8, device=self.device)
+                d.copy_(staged[1], non_blocking=True)
                 rc = self.lib.rbim_init_spins(ctypes.c_void_p(d.data_ptr()), chains,
                                               ctypes.c_void_p(self.word_pool.data_ptr()), int(plan.hot),
                                               ctypes.c_void_p(self.stream.cuda_stream))
                 _native.check(rc, "rbim_init_spins")
             n_total = plan.n_therm + plan.n_bins * plan.sweeps_per_bin
             self._active.append(_Active(p.req, plan, p.future, p.submitted, time.perf_counter(), spin_off, coup_off,
-                                        words, r_off, chains * plan.n_bins, desc, n_total))
+                                        words, r_off, chains * plan.n_bins, desc, n_total, staged=(staged, d)))
             n_chains += chains
 
     def _launch(self) -> None:
@@ -332,104 +355,125 @@ class ScanServer:
         pool = ctypes.c_void_p(self.word_pool.data_ptr())
         ai, af = ctypes.c_void_p(self.acc_int.data_ptr()), ctypes.c_void_p(self.acc_f64.data_ptr())
         live = [a for a in self._active if a.done < a.n_total]
-        resident = [a for a in live if a.plan.L <= self.resident_max_l]
-        clustered = [a for a in live if self.resident_max_l < a.plan.L <= self.cluster_max_l]
-        plain = [a for a in live if a.plan.L > max(self.resident_max_l, self.cluster_max_l)]
-        descs = [a.desc for a in resident] + [a.desc for a in clustered] + [a.desc for a in plain]
-        if not descs:
+        if not live:
             return
-        allc = np.concatenate(descs)
+        buckets: Dict[tuple, List[_Active]] = {}
+        for a, key in zip(live, _native.engine_buckets([a.plan.L for a in live], self.resident_max_l,
+                                                       self.cluster_max_l)):
+            buckets.setdefault(key, []).append(a)
+        keys = sorted(buckets)
+        allc = np.concatenate([a.desc for k in keys for a in buckets[k]])
         # The previous launch's descriptor copy must have left the pinned buffer.
         self._desc_copied.synchronize()
         host = self.desc_host.numpy()[: 96 * len(allc)]
         host[:] = allc.view(np.uint8)
         n = len(allc)
+        st = ctypes.c_void_p(self.status.data_ptr())
+        qw = ctypes.c_void_p(self.queue_ws.data_ptr())
         with torch.cuda.stream(self.stream):
             self.desc_dev[: 96 * n].copy_(self.desc_host[: 96 * n], non_blocking=True)
             self._desc_copied.record(self.stream)
-            n_res = sum(len(a.desc) for a in resident)
-            if n_res:
-                l_max = max(a.plan.L for a in resident)
-                rc = self.lib.rbim_sweeps_batched(ctypes.c_void_p(self.desc_dev.data_ptr()), n_res, l_max, pool, pool,
-                                                  ai, af, None, self.quantum, self.threads,
-                                                  ctypes.c_void_p(self.status.data_ptr()),
-                                                  ctypes.c_void_p(self.queue_ws.data_ptr()), self.queue_ws.numel(), sp)
-                _native.check(rc, "rbim_sweeps_batched")
-                self.launches += 1
-            n_clu = sum(len(a.desc) for a in clustered)
-            if n_clu:
-                l_max = max(a.plan.L for a in clustered)
-                rc = self.lib.rbim_sweeps_clustered(ctypes.c_void_p(self.desc_dev.data_ptr() + 96 * n_res), n_clu,
-                                                    l_max, pool, pool, ai, af, None, self.quantum,
-                                                    ctypes.c_void_p(self.status.data_ptr()),
-                                                    ctypes.c_void_p(self.queue_ws.data_ptr()), self.queue_ws.numel(),
-                                                    sp)
-                _native.check(rc, "rbim_sweeps_clustered")
-                self.launches += 1
-            if plain:
-                l_big = max(a.plan.L for a in plain)
-                need = int(self.lib.rbim_plain_workspace_bytes(l_big))
-                if self._plain_ws is None or self._plain_ws.numel() < need:
-                    self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
-                base = self.desc_dev.data_ptr() + 96 * (n_res + n_clu)
-                k = 0
-                for a in plain:
-                    for _ in range(len(a.desc)):
-                        rc = self.lib.rbim_sweeps_plain(a.plan.L, ctypes.c_void_p(base + 96 * k), pool, pool, ai, af,
-                                                        None, self.quantum, ctypes.c_void_p(self.status.data_ptr()),
+            first = 0
+            for key in keys:
+                group = buckets[key]
+                count = sum(len(a.desc) for a in group)
+                l_max = max(a.plan.L for a in group)
+                base = self.desc_dev.data_ptr() + 96 * first
+                if key[0] == 0:
+                    rc = self.lib.rbim_sweeps_batched(ctypes.c_void_p(base), count, l_max, pool, pool, ai, af, None,
+                                                      self.quantum, self.threads, st, qw, self.queue_ws.numel(), sp)
+                    _native.check(rc, "rbim_sweeps_batched")
+                    self.launches += 1
+                elif key[0] == 1:
+                    rc = self.lib.rbim_sweeps_clustered(ctypes.c_void_p(base), count, l_max, pool, pool, ai, af,
+                                                        None, self.quantum, st, qw, self.queue_ws.numel(), sp)
+                    _native.check(rc, "rbim_sweeps_clustered")
+                    self.launches += 1
+                else:
+                    need = int(self.lib.rbim_plain_workspace_bytes(l_max))
+                    if self._plain_ws is None or self._plain_ws.numel() < need:
+                        self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+                    for k in range(count):
+                        rc = self.lib.rbim_sweeps_plain(int(allc["L"][first + k]), ctypes.c_void_p(base + 96 * k),
+                                                        pool, pool, ai, af, None, self.quantum, st,
                                                         ctypes.c_void_p(self._plain_ws.data_ptr()),
                                                         self._plain_ws.numel(), sp)
                         _native.check(rc, "rbim_sweeps_plain")
                         self.launches += 1
-                        k += 1
+                first += count
+        finished = []
         for a in live:
             a.done = min(a.n_total, a.done + self.quantum)
             a.desc["sweep"] = a.done
+            if a.done >= a.n_total:
+                finished.append(a)
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self._inflight.append((ev, finished))
 
-    def _retire(self) -> None:
-        """Bring back and assemble every finished request; free its pool ranges."""
-        finished = [a for a in self._active if a.done >= a.n_total]
-        if not finished:
-            return
+    def _retire(self, block: bool) -> None:
+        """Bring back and assemble the requests of completed launches; free their pool ranges.
+
+        The sums of a launch are copied on a side stream once that launch's
+        event has fired, so the next launch keeps the device busy meanwhile.
+        With ``block`` the oldest launch in flight is waited for.
+        """
         torch = _torch()
-        self.stream.synchronize()
-        st = int(self.status.item())
-        if st:
-            raise _native.RbimError(f"device status word {st:#x} (1 = find bound, 2 = union bound, 4 = bad chain)")
-        for a in finished:
-            with torch.cuda.stream(self.stream):
-                ib = self.acc_int[a.row_off: a.row_off + a.rows].cpu().numpy()
-                fb = self.acc_f64[a.row_off: a.row_off + a.rows].cpu().numpy()
-            nb = a.plan.n_bins
-            result = assemble_scan(a.plan, ib.reshape(-1, nb, _native.ACC_INT), fb.reshape(-1, nb, _native.ACC_F64))
-            now = time.perf_counter()
-            self.words.release(a.spin_off, a.words)
-            self.rows.release(a.row_off, a.rows)
-            self._active.remove(a)
-            self.completed.append({"L": a.plan.L, "chains": len(a.desc), "sweeps": a.n_total,
-                                   "site_updates": len(a.desc) * a.n_total * a.plan.L * a.plan.L,
-                                   "submitted": a.submitted, "admitted": a.admitted, "finished": now,
-                                   "latency": now - a.submitted})
-            a.future.set_result(result)
-            self._inbox.task_done()
+        while self._inflight:
+            ev, finished = self._inflight[0]
+            if not ev.query():
+                if not block:
+                    return
+                ev.synchronize()
+            self._inflight.pop(0)
+            block = False
+            copies = []
+            with torch.cuda.stream(self.copy_stream):
+                self.copy_stream.wait_event(ev)
+                status = self.status.to("cpu", non_blocking=True)
+                for a in finished:
+                    copies.append((self.acc_int[a.row_off: a.row_off + a.rows].to("cpu", non_blocking=True),
+                                   self.acc_f64[a.row_off: a.row_off + a.rows].to("cpu", non_blocking=True)))
+            self.copy_stream.synchronize()
+            st = int(status.item())
+            if st:
+                raise _native.RbimError(f"device status word {st:#x} (1 = find bound, 2 = union bound, 4 = bad chain)")
+            for a, (ib, fb) in zip(finished, copies):
+                nb = a.plan.n_bins
+                result = assemble_scan(a.plan, ib.numpy().reshape(-1, nb, _native.ACC_INT),
+                                       fb.numpy().reshape(-1, nb, _native.ACC_F64))
+                now = time.perf_counter()
+                self.words.release(a.spin_off, a.words)
+                self.rows.release(a.row_off, a.rows)
+                self._active.remove(a)
+                self.completed.append({"L": a.plan.L, "chains": len(a.desc), "sweeps": a.n_total,
+                                       "site_updates": len(a.desc) * a.n_total * a.plan.L * a.plan.L,
+                                       "submitted": a.submitted, "admitted": a.admitted, "finished": now,
+                                       "latency": now - a.submitted})
+                a.future.set_result(result)
+                self._inbox.task_done()
 
     def step(self) -> bool:
-        """Admit, launch one quantum, retire finished requests.  Returns False when there is nothing to run."""
+        """Admit, launch one quantum, retire what earlier launches finished.
+
+        At most two launches are in flight: while one runs, the host admits,
+        enqueues the next and retires the one before.  Returns False when there
+        is nothing to run or to retire.
+        """
         self._drain_inbox()
         self._admit()
-        if not self._active:
+        launched = any(a.done < a.n_total for a in self._active)
+        if launched:
+            self._launch()
+        if not launched and not self._inflight:
             return False
-        self._launch()
-        # Plan the next waiting request on the host while the launch runs.
-        if self._waiting and self._waiting[0].plan is None:
-            self._waiting[0].plan = self._waiting[0].req.plan()
-        self._retire()
+        self._retire(block=len(self._inflight) > 1 or not launched)
         return True
 
     def run_until_idle(self) -> None:
         """Drive the loop on the calling thread until every submitted request has finished."""
         while True:
-            if not self.step() and self._inbox.empty() and not self._waiting:
+            if not self.step() and self._inbox.empty() and not self._waiting and not self._inflight:
                 return
 
     def latency_percentiles(self, qs=(50, 99)) -> Dict[str, float]:

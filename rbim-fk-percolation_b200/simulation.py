@@ -358,20 +358,58 @@ def run_scan_tasks(plan: ScanPlan, tasks: Optional[Sequence[int]] = None, *, eng
 
 
 def assemble_scan(plan: ScanPlan, int_sums: np.ndarray, f_sums: np.ndarray) -> Dict[str, object]:
-    """Jackknife-combined observables and metadata from every task's sums (reference ``simulation.py:401-444``)."""
+    """Jackknife-combined observables and metadata from every task's sums (reference ``simulation.py:401-444``).
+
+    The estimators of :func:`combine_realizations` (per-realization full-run
+    and per-bin means, disorder average, leave-one-out jackknife, bin-based
+    thermal error), evaluated for all temperatures at once.
+    """
     n_r = plan.n_realizations
     temperatures = plan.temperatures
-    raw = [realization_from_sums(int_sums[k], f_sums[k], plan.sweeps_per_bin, plan.measure_percolation)
-           for k in range(plan.n_tasks)]
+    n_t, nb, spb = len(temperatures), plan.n_bins, plan.sweeps_per_bin
+    total = nb * spb
     n_sites = plan.L * plan.L
-    results = {name: {"value": np.empty(len(temperatures)), "error": np.empty(len(temperatures)),
-                      "thermal_error": np.empty(len(temperatures))} for name in OBSERVABLES}
-    for t_index, temperature in enumerate(temperatures):
-        block = raw[t_index * n_r:(t_index + 1) * n_r]
-        combined = combine_realizations(block, temperature, n_sites)
+    ii = np.asarray(int_sums).reshape(n_t, n_r, nb, -1)
+    ff = np.asarray(f_sums, dtype=np.float64).reshape(n_t, n_r, nb, -1)
+    prim: Dict[str, np.ndarray] = {}
+    bins: Dict[str, np.ndarray] = {}
+    for name in PRIMITIVES:
+        kind, k = _SOURCE[name]
+        if not plan.measure_percolation and name.startswith("wrap"):
+            prim[name] = np.full((n_t, n_r), np.nan)
+            bins[name] = np.full((n_t, n_r, nb), np.nan)
+        elif kind == "i":
+            col = ii[..., k]
+            prim[name] = col.sum(axis=2).astype(np.float64) / total
+            bins[name] = col.astype(np.float64) / spb
+        else:
+            col = np.ascontiguousarray(ff[..., k])
+            prim[name] = col.sum(axis=2) / total
+            bins[name] = col / spb
+    temps = np.asarray(temperatures, dtype=np.float64)
+    results = {name: {"value": np.empty(n_t), "error": np.full(n_t, np.nan), "thermal_error": np.full(n_t, np.nan)}
+               for name in OBSERVABLES}
+    if n_t and n_r:
+        central = derive_observables({name: v.mean(axis=1) for name, v in prim.items()}, temps, n_sites)
         for name in OBSERVABLES:
-            for key in ("value", "error", "thermal_error"):
-                results[name][key][t_index] = combined[name][key]
+            results[name]["value"][:] = central[name]
+        if n_r > 1:
+            loo = {name: (v.sum(axis=1, keepdims=True) - v) / (n_r - 1) for name, v in prim.items()}
+            derived = derive_observables(loo, temps[:, None], n_sites)
+            factor = (n_r - 1) / n_r
+            for name in OBSERVABLES:
+                samples = np.broadcast_to(np.asarray(derived[name], dtype=float), (n_t, n_r))
+                dev = samples - samples.mean(axis=1, keepdims=True)
+                results[name]["error"][:] = np.sqrt(factor * np.sum(dev * dev, axis=1))
+        if nb > 1:
+            derived = derive_observables(bins, temps[:, None, None], n_sites)
+            for name in OBSERVABLES:
+                values = np.broadcast_to(np.asarray(derived[name], dtype=float), (n_t, n_r, nb))
+                spread = np.std(values, axis=2, ddof=1) / np.sqrt(nb)
+                results[name]["thermal_error"][:] = np.sqrt(np.mean(spread**2, axis=1) / n_r)
+        if n_r == 1:
+            for name in OBSERVABLES:
+                results[name]["error"][:] = results[name]["thermal_error"]
 
     metadata = {
         "L": plan.L,

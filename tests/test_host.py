@@ -203,3 +203,43 @@ def test_engine_refuses_to_run_without_cuda(rb):
         pytest.skip("a CUDA device is present")
     with pytest.raises(rb.RbimError):
         rb.run_temperature_scan(8, 0.1, [2.0], n_sweeps=20, n_bins=2)
+
+
+def _per_temperature_assembly(rb, plan, int_sums, f_sums):
+    """The per-temperature path: realization_from_sums and combine_realizations, one temperature at a time."""
+    n_r = plan.n_realizations
+    raw = [rb.realization_from_sums(int_sums[k], f_sums[k], plan.sweeps_per_bin, plan.measure_percolation)
+           for k in range(plan.n_tasks)]
+    out = {}
+    for t, T in enumerate(plan.temperatures):
+        out[t] = rb.combine_realizations(raw[t * n_r:(t + 1) * n_r], T, plan.L * plan.L)
+    return out
+
+
+@pytest.mark.parametrize("n_r,n_bins,measure", [(5, 4, True), (1, 6, True), (3, 1, False), (7, 10, True)])
+def test_vectorised_assembly_matches_per_temperature(rb, n_r, n_bins, measure):
+    rng = np.random.default_rng(n_r * 100 + n_bins)
+    L, spb = 12, 9
+    temps = [1.3, 2.1, 2.6, 3.4]
+    plan = rb.ScanPlan(L=L, p=0.1, temperatures=temps, couplings=[np.ones(2 * L * L, np.int8)] * n_r,
+                       keys=np.arange(len(temps) * n_r, dtype=np.uint64), n_sweeps=n_bins * spb, n_therm=3,
+                       n_bins=n_bins, sweeps_per_bin=spb, seed=1, hot=True, start="hot", measure_percolation=measure)
+    N = L * L
+    n = plan.n_tasks
+    E = rng.integers(-2 * N, 0, size=(n, n_bins, spb))
+    M = rng.integers(-N, N + 1, size=(n, n_bins, spb))
+    S1 = rng.integers(1, N + 1, size=(n, n_bins, spb))
+    MC = rng.integers(0, N + 1, size=(n, n_bins, spb))
+    S2 = rng.integers(0, N // 2, size=(n, n_bins, spb))
+    NC = rng.integers(1, N, size=(n, n_bins, spb))
+    WX = rng.integers(0, 2, size=(n, n_bins, spb))
+    WY = rng.integers(0, 2, size=(n, n_bins, spb))
+    ii = np.stack([E.sum(-1), (E * E).sum(-1), M.sum(-1), np.abs(M).sum(-1), (M * M).sum(-1), S1.sum(-1), MC.sum(-1),
+                   S2.sum(-1), NC.sum(-1), WX.sum(-1), WY.sum(-1), (WX | WY).sum(-1)], axis=-1).astype(np.int64)
+    ff = np.stack([((M * M).astype(float) ** 2).sum(-1), (MC / S1).sum(-1)], axis=-1)
+    got = rb.assemble_scan(plan, ii, ff)["observables"]
+    want = _per_temperature_assembly(rb, plan, ii, ff)
+    for name in rb.OBSERVABLES:
+        for field in ("value", "error", "thermal_error"):
+            w = np.array([want[t][name][field] for t in range(len(temps))])
+            np.testing.assert_allclose(got[name][field], w, rtol=1e-12, atol=1e-15, err_msg=f"{name} {field}")
