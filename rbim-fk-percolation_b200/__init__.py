@@ -55,6 +55,7 @@ from .simulation import (
 )
 from .serving import RangeAllocator, ScanRequest, ScanServer, request_footprint
 from .sharding import gather_task_sums, run_temperature_scan_sharded, shard_bounds
+from .timeseries import collect_series, integrated_autocorrelation
 from .swendsen_wang import SweepResult, aligned_spins, energy, initial_spins, magnetization, random_spins, sw_sweep
 
 __version__ = "0.1.0"
@@ -105,6 +106,8 @@ __all__ = [
     "ScanServer",
     "RangeAllocator",
     "request_footprint",
+    "collect_series",
+    "integrated_autocorrelation",
     "save_results",
     "load_results",
     "ChainSet",
