@@ -39,7 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_SITE_UPDATE = 8.5  # packed spins r+w, packed couplings r, one int32 cluster id w+r
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_resident_sweeps_L256.txt")
+PROFILES = os.path.join(ROOT, "profiles")
 
 
 def workload(name: str):
@@ -53,6 +53,16 @@ def workload(name: str):
         ps = [0.05]
         n_real = 256
         temps = np.linspace(1.0, 3.0, 64)
+    elif name == "c4_L512":
+        L = 512
+        ps = [0.02, 0.05, 0.08, 0.10]
+        n_real = int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
+        temps = np.linspace(1.2, 2.4, 32)
+    elif name == "c2_L1024":
+        L = 1024
+        ps = [0.10]
+        n_real = 4
+        temps = np.linspace(1.5, 1.7, 32)
     else:
         raise SystemExit(f"unknown workload {name}")
     return L, ps, n_real, temps
@@ -142,10 +152,10 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch of the resident kernel from the committed ncu summary, or None."""
+def profiled_traffic(path):
+    """DRAM bytes per launch of the workload's kernel from the committed ncu summary, or None."""
     try:
-        with open(PROFILE_TRAFFIC) as f:
+        with open(path) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_launch_scaled:"):
                     return float(line.split(":", 1)[1])
@@ -403,7 +413,8 @@ def main():
     site_updates_launch = n_chains * S * L * L
     peak, peak_kind = measured_peak_hbm()
     achieved = BYTES_PER_SITE_UPDATE * site_updates_launch / launch_s / 1e9
-    traffic = profiled_traffic()
+    kernel = "k_resident_sweeps" if L <= rb._native.resident_max_l() else "k_cluster_sweeps"
+    traffic = profiled_traffic(os.path.join(PROFILES, f"{kernel}_L{L}.txt"))
 
     # Plain engine: one lattice per launch sequence, same L.
     plain = None
@@ -493,12 +504,13 @@ def main():
         "data": "synthetic (seeded +-J disorder from the reference's generator)",
         "config": {"workload": args.workload, "L": L, "p": ps, "realizations_per_p": n_real,
                    "temperatures": [float(temps[0]), float(temps[-1]), len(temps)], "chains_per_gpu": n_chains,
-                   "sweeps_per_step": S, "measured": True, "engine": "resident (batched)",
+                   "sweeps_per_step": S, "measured": True,
+                   "engine": "resident (batched)" if kernel == "k_resident_sweeps" else "cluster (batched)",
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"independent chains x{world}"},
         "site_updates_per_s": value * L * L,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "bytes_per_site_update": BYTES_PER_SITE_UPDATE, "kernel": "k_resident_sweeps"},
+                     "bytes_per_site_update": BYTES_PER_SITE_UPDATE, "kernel": kernel},
         "clocks": clocks.summary(),
         "gpu_launches": args.steps,
         "e2e": e2e,
