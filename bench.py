@@ -209,6 +209,21 @@ def config_lines(rb, dev, seed):
     the L = 512 slice of the uneven-size mix and L = 1024 (cluster engine), one L = 1024 lattice."""
     out = {}
 
+    # The reference's own headline scan (plain method, small): L = 32, p = 0.05, 32 realizations x 40 T,
+    # 20,000 measured + 2,000 thermalisation sweeps, 20 bins, end to end through run_temperature_scan.
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rb.run_temperature_scan(32, 0.05, np.linspace(1.0, 3.0, 40), n_realizations=32, n_sweeps=20000, n_therm=2000,
+                            n_bins=20, seed=0, device=dev, chunk=5000)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    sweeps = 32 * 40 * 22000
+    out["c1_L32_scan"] = {"wall_s": wall, "lattice_sweeps_per_s": sweeps / wall,
+                          "site_updates_per_s": sweeps * 1024 / wall, "chains": 1280, "sweeps_per_chain": 22000,
+                          "api": "run_temperature_scan, host disorder, copies and jackknife included"}
+
     def chainset(L, p, n_real, temps, n_total, s):
         specs, couplings = build_chains(rb, L, [p], n_real, temps, s, n_total)
         cs = rb.ChainSet(specs, couplings, device=dev)
@@ -333,7 +348,7 @@ def main():
     ap.add_argument("--workload", default="c4_L256")
     ap.add_argument("--sweeps-per-step", type=int, default=5)
     ap.add_argument("--threads", type=int, default=0, help="resident CTA size (0 = default)")
-    ap.add_argument("--e2e-sweeps", type=int, default=40)
+    ap.add_argument("--e2e-sweeps", type=int, default=200)
     ap.add_argument("--plain-sweeps", type=int, default=200)
     ap.add_argument("--ref-seconds", type=float, default=3.0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
