@@ -12,8 +12,13 @@
 #include "rbim_phases.cuh"
 
 #ifndef RBIM_COUNT
+#ifdef RBIM_PROFILE_PHASES
+#define RBIM_COUNT(k, v) ((void)(v))
+#define RBIM_PROF_ONLY(...) __VA_ARGS__
+#else
 #define RBIM_COUNT(k, v) ((void)0)
 #define RBIM_PROF_ONLY(...)
+#endif
 #endif
 
 namespace rbim {
