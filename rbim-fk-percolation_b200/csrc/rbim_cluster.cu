@@ -539,6 +539,19 @@ __device__ __forceinline__ uint32_t node_root(const Ctx &x, uint32_t k)
     return *((volatile uint32_t *)(x.HW + k));
 }
 
+// The open-tile union and root walks as separate (non-inlined) functions: the
+// cluster kernel keeps more state live across its phases than the resident
+// one, and compiled inline these pointer-chasing loops lose registers to it.
+static __device__ __noinline__ void cluster_union(const Lat<Word16> &t, uint32_t tid)
+{
+    phase_union_open(t, tid, kCT);
+}
+
+static __device__ __noinline__ void cluster_roots(const Lat<Word16> &t, uint32_t tid)
+{
+    (void)phase_roots_flat(t, tid, kCT);
+}
+
 __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g)
 {
     return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
@@ -624,9 +637,9 @@ __global__ void __launch_bounds__(kCT, 1)
                 x.HW[k] = Word64::make((c << 16) | k, 0, 0);
             }
             __syncthreads();
-            phase_union_open(t, tid, kCT);
+            cluster_union(t, tid);
             __syncthreads();
-            (void)phase_roots_flat(t, tid, kCT);
+            cluster_roots(t, tid);
             __syncthreads();
             cl.sync();  // every tile's roots are final
 
