@@ -34,9 +34,9 @@ constexpr uint32_t kMaxResidentSites = 65536;  // 16-bit parents
 constexpr size_t kMaxSmem = 227 * 1024 - 8 * 1024;
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 
-size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+__host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-uint32_t hash_size(uint32_t l_max)
+__host__ __device__ constexpr uint32_t hash_size(uint32_t l_max)
 {
     // At most 4L distinct open roots touch a seam bond; keep the load <= 1/2.
     uint32_t h = 32;
@@ -90,9 +90,11 @@ struct SeamWord {
     __device__ __forceinline__ static bool nonzero(int v) { return (v & 0x3FF) != 0; }
 };
 
-ResidentLayout resident_layout(uint32_t l_max, int threads)
+// Shared-memory layout for lattices of up to l_max x l_max sites; constexpr so
+// that the launches of the common size classes get it as a compile-time
+// constant (the kernel's shared-memory views then need no registers).
+__host__ __device__ constexpr ResidentLayout resident_layout_c(uint32_t l_max)
 {
-    (void)threads;
     ResidentLayout ly{};
     ly.l_max = l_max;
     ly.n_max = l_max * l_max;
@@ -127,6 +129,12 @@ ResidentLayout resident_layout(uint32_t l_max, int threads)
     off += 4ull * ly.hs;
     ly.bytes = align16(off);
     return ly;
+}
+
+ResidentLayout resident_layout(uint32_t l_max, int threads)
+{
+    (void)threads;
+    return resident_layout_c(l_max);
 }
 
 int resident_max_l()
@@ -471,12 +479,16 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
     __syncthreads();
 }
 
-template <int NT>
+// LC > 0: the launch's layout is resident_layout_c(LC), a compile-time
+// constant; LC == 0: the layout passed in.
+template <int NT, int LC>
 __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
     k_resident_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, const uint32_t *coupling_pool,
                       long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *queue, int *status,
-                      ResidentLayout ly)
+                      ResidentLayout ly_arg)
 {
+    constexpr ResidentLayout kly = resident_layout_c(LC > 0 ? LC : 16);
+    const ResidentLayout ly = LC > 0 ? kly : ly_arg;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Red<NT> red;
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -650,30 +662,50 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
 
 namespace {
 
-template <int NT>
-cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
+template <int NT, int LC>
+cudaError_t launch_sweeps_lc(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                              const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
                              int n_sweeps, int grid, int *queue, int *status, cudaStream_t stream)
 {
-    const ResidentLayout ly = resident_layout(l_max, NT);
-    cudaError_t e = cudaFuncSetAttribute(k_resident_sweeps<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const ResidentLayout ly = LC > 0 ? resident_layout_c(LC) : resident_layout(l_max, NT);
+    cudaError_t e = cudaFuncSetAttribute(k_resident_sweeps<NT, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ly.bytes);
     if (e != cudaSuccess) return e;
     if (grid <= 0) {
         int per_sm = 0, sms = 0, dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident_sweeps<NT>, NT, ly.bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident_sweeps<NT, LC>, NT, ly.bytes);
         if (e != cudaSuccess) return e;
         grid = std::max(1, per_sm) * sms;
     }
     grid = std::min(grid, n_chains);
     e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
     if (e != cudaSuccess) return e;
-    k_resident_sweeps<NT><<<grid, NT, ly.bytes, stream>>>(const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
+    k_resident_sweeps<NT, LC><<<grid, NT, ly.bytes, stream>>>(const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
                                                           coupling_pool, acc_i, acc_f, rec, n_sweeps, queue,
                                                           status, ly);
     return cudaGetLastError();
+}
+
+// Size classes with a compile-time layout: the default thread counts of
+// 128 < L <= 256 and 64 < L <= 128 (1024 threads) and 32 < L <= 64 (512).
+template <int NT>
+cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
+                             const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
+                             int n_sweeps, int grid, int *queue, int *status, cudaStream_t stream)
+{
+    if (NT == 1024 && l_max > 128 && l_max <= 256)
+        return launch_sweeps_lc<NT, 256>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                         n_sweeps, grid, queue, status, stream);
+    if (NT == 1024 && l_max > 64 && l_max <= 128)
+        return launch_sweeps_lc<NT, 128>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                         n_sweeps, grid, queue, status, stream);
+    if (NT == 512 && l_max > 32 && l_max <= 64)
+        return launch_sweeps_lc<NT, 64>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                        n_sweeps, grid, queue, status, stream);
+    return launch_sweeps_lc<NT, 0>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
+                                   grid, queue, status, stream);
 }
 
 template <int NT>
