@@ -51,7 +51,7 @@ constexpr uint32_t kSlotsPerThread = 4; // hash size <= 4 * kCT
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
 constexpr size_t kSmemBudget = 227 * 1024 - 4 * 1024;
 
-size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
+__host__ __device__ constexpr size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
 
 }  // namespace
 
@@ -64,7 +64,7 @@ uint32_t cluster_size_for(uint32_t L)
 
 namespace {
 
-uint32_t cluster_hash_size(uint32_t l_max, uint32_t T)
+__host__ __device__ constexpr uint32_t cluster_hash_size(uint32_t l_max, uint32_t T)
 {
     // Tile roots that can touch a boundary bond: the first and last L sites,
     // the row ends and row starts of the tile's rows, the tile-end site.
@@ -77,7 +77,10 @@ uint32_t cluster_hash_size(uint32_t l_max, uint32_t T)
 
 }  // namespace
 
-ClusterLayout cluster_layout(uint32_t l_max, uint32_t C)
+// Shared-memory layout of one CTA's tile for lattices of up to l_max sites
+// across C CTAs; constexpr so that the common classes get it as a
+// compile-time constant.
+__host__ __device__ constexpr ClusterLayout cluster_layout_c(uint32_t l_max, uint32_t C)
 {
     ClusterLayout ly{};
     ly.l_max = l_max;
@@ -108,6 +111,8 @@ ClusterLayout cluster_layout(uint32_t l_max, uint32_t C)
     ly.bytes = a16(off);
     return ly;
 }
+
+ClusterLayout cluster_layout(uint32_t l_max, uint32_t C) { return cluster_layout_c(l_max, C); }
 
 bool cluster_layout_fits(const ClusterLayout &ly)
 {
@@ -557,17 +562,22 @@ __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g
     return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
 }
 
+// LC > 0: the layout is cluster_layout_c(LC, CC), a compile-time constant,
+// and the cluster has CC CTAs; LC == 0: the layout passed in.
+template <int LC, int CC>
 __global__ void __launch_bounds__(kCT, 1)
     k_cluster_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, const uint32_t *coupling_pool,
                      long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *queue, int *status,
-                     ClusterLayout ly)
+                     ClusterLayout ly_arg)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ CRed red;
+    constexpr ClusterLayout kly = cluster_layout_c(LC > 0 ? LC : 512, CC > 0 ? CC : 4);
+    const ClusterLayout ly = LC > 0 ? kly : ly_arg;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     constexpr uint32_t nwarps = kCT / 32;
-    const uint32_t C = cl.num_blocks(), c = cl.block_rank();
+    const uint32_t C = CC > 0 ? (uint32_t)CC : cl.num_blocks(), c = cl.block_rank();
 
     if (tid == 0) red.err = 0;
     for (;;) {
@@ -901,15 +911,16 @@ __global__ void __launch_bounds__(kCT, 1)
 
 }  // namespace
 
-cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters)
+namespace {
+
+template <int LC, int CC>
+cudaError_t occupancy_t(const ClusterLayout &ly, uint32_t C, int *clusters)
 {
-    *clusters = 0;
-    const ClusterLayout ly = cluster_layout(l_max, C);
-    if (!cluster_layout_fits(ly)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_cluster_sweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ly.bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_cluster_sweeps<LC, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ly.bytes);
     if (e != cudaSuccess) return e;
     if (C > 8u) {
-        e = cudaFuncSetAttribute(k_cluster_sweeps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        e = cudaFuncSetAttribute(k_cluster_sweeps<LC, CC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
     }
     cudaLaunchConfig_t cfg = {};
@@ -923,20 +934,18 @@ cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters)
     cfg.dynamicSmemBytes = ly.bytes;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(clusters, k_cluster_sweeps, &cfg);
+    return cudaOccupancyMaxActiveClusters(clusters, k_cluster_sweeps<LC, CC>, &cfg);
 }
 
-cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
-                                  const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
-                                  int n_sweeps, int *queue, int *status, cudaStream_t stream)
+template <int LC, int CC>
+cudaError_t launch_t(const ClusterLayout &ly, uint32_t C, const rbim_chain_t *chains, int n_chains,
+                     uint32_t *spin_pool, const uint32_t *coupling_pool, long long *acc_i, double *acc_f,
+                     int32_t *rec, int n_sweeps, int *queue, int *status, cudaStream_t stream)
 {
-    const uint32_t C = cluster_size_for((uint32_t)l_max);
-    if (C == 0) return cudaErrorInvalidValue;
     int clusters = 0;
-    cudaError_t e = cluster_occupancy((uint32_t)l_max, C, &clusters);
+    cudaError_t e = occupancy_t<LC, CC>(ly, C, &clusters);
     if (e != cudaSuccess) return e;
     if (clusters <= 0) return cudaErrorInvalidConfiguration;
-    const ClusterLayout ly = cluster_layout((uint32_t)l_max, C);
     const int n_clusters = std::min(clusters, n_chains);
     e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
     if (e != cudaSuccess) return e;
@@ -952,10 +961,51 @@ cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int 
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_cluster_sweeps, const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
+    e = cudaLaunchKernelEx(&cfg, k_cluster_sweeps<LC, CC>, const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
                            coupling_pool, acc_i, acc_f, rec, n_sweeps, queue, status, ly);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+// The classes with a compile-time layout: 4-CTA clusters up to L = 512 and
+// 16-CTA clusters up to L = 1024 (the largest lattices of those sizes).
+int layout_class(uint32_t l_max, uint32_t C)
+{
+    if (C == 4u && l_max <= 512u && cluster_size_for(512u) == 4u) return 512;
+    if (C == 16u && l_max <= 1024u && cluster_size_for(1024u) == 16u) return 1024;
+    return 0;
+}
+
+}  // namespace
+
+cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters)
+{
+    *clusters = 0;
+    const int lc = layout_class(l_max, C);
+    const ClusterLayout ly = lc ? cluster_layout((uint32_t)lc, C) : cluster_layout(l_max, C);
+    if (!cluster_layout_fits(ly)) return cudaSuccess;
+    if (lc == 512) return occupancy_t<512, 4>(ly, C, clusters);
+    if (lc == 1024) return occupancy_t<1024, 16>(ly, C, clusters);
+    return occupancy_t<0, 0>(ly, C, clusters);
+}
+
+cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
+                                  const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
+                                  int n_sweeps, int *queue, int *status, cudaStream_t stream)
+{
+    const uint32_t C = cluster_size_for((uint32_t)l_max);
+    if (C == 0) return cudaErrorInvalidValue;
+    const int lc = layout_class((uint32_t)l_max, C);
+    const ClusterLayout ly = lc ? cluster_layout((uint32_t)lc, C) : cluster_layout((uint32_t)l_max, C);
+    if (!cluster_layout_fits(ly)) return cudaErrorInvalidConfiguration;
+    if (lc == 512)
+        return launch_t<512, 4>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
+                                queue, status, stream);
+    if (lc == 1024)
+        return launch_t<1024, 16>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
+                                  queue, status, stream);
+    return launch_t<0, 0>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps, queue,
+                          status, stream);
 }
 
 }  // namespace rbim

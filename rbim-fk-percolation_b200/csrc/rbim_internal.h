@@ -47,14 +47,14 @@ struct ClusterLayout {
 
 // Tile size of an N-site lattice split over C CTAs: ceil(N / C) rounded up to
 // a multiple of 128 sites, so that tiles start on Philox chunk boundaries.
-__host__ __device__ inline uint32_t cluster_tile_size(uint32_t N, uint32_t C)
+__host__ __device__ constexpr uint32_t cluster_tile_size(uint32_t N, uint32_t C)
 {
     const uint32_t t = (N + C - 1u) / C;
     return (t + 127u) & ~127u;
 }
 
 // C tiles fit an L x L lattice when every tile holds between L and 65536 sites.
-__host__ __device__ inline bool cluster_tiles_ok(uint32_t L, uint32_t C)
+__host__ __device__ constexpr bool cluster_tiles_ok(uint32_t L, uint32_t C)
 {
     const uint32_t N = L * L, T = cluster_tile_size(N, C);
     if (T > 65536u || T < L) return false;
