@@ -709,20 +709,8 @@ __global__ void __launch_bounds__(kCT, 1)
             }
             __syncthreads();
             // Tile piece sizes minus one into the tile roots' words (a tile
-            // piece may hold all 65536 sites): every run piece adds its
-            // length, the piece that starts at the root one less.
-            for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
-                const uint32_t valid = t.g.valid(w);
-                const uint32_t lead = piece_leaders(t, w, valid);
-                if ((lead >> lane) & 1u) {
-                    const uint32_t n = (w << 5) + lane;
-                    const uint32_t next = lead & ~mask_le(lane);
-                    const uint32_t end = next ? (uint32_t)(__ffs(next) - 1) : (uint32_t)__popc(valid);
-                    const bool is_root = (t.ROOT[w] >> lane) & 1u;
-                    const uint32_t r = is_root ? n : (uint32_t)u16[n];
-                    add16(u16, r, end - lane - (is_root ? 1u : 0u));
-                }
-            }
+            // piece may hold all 65536 sites).
+            count_pieces<true>(t, u16, warp, nwarps);
             __syncthreads();
             // OV (no longer needed this sweep) becomes the plane of node marks.
             for (uint32_t w = tid; w < t.g.NW; w += kCT) t.OV[w] = 0u;

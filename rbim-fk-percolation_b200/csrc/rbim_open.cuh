@@ -285,4 +285,64 @@ __device__ __forceinline__ void add16(unsigned short *base, uint32_t i, uint32_t
     atomicAdd((unsigned int *)(base + (i & ~1u)), v << (16u * (i & 1u)));
 }
 
+// Cluster sizes into the root words (after the sites pass, every non-root
+// site's word holds its root): one add per run piece, the sites of a word
+// split into maximal runs sharing a root.  With at least 32 words per warp,
+// each lane takes a word of its warp's block of 32 and walks the word's
+// pieces, summing consecutive pieces of one root in a register; at the end
+// of the block the lanes holding the same root add their sums in one atomic,
+// so a giant cluster sees one add per block instead of one per piece.
+// kMinusOne: the piece that starts at the root adds one less, so that a root
+// word holds size - 1 (a tile of 65536 sites then still fits 16 bits).
+// Root words must be zero on entry.
+template <bool kMinusOne>
+__device__ __forceinline__ void count_pieces(const Lat<Word16> &t, unsigned short *u16, uint32_t warp,
+                                             uint32_t nwarps)
+{
+    const Geom &g = t.g;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (g.NW >= 32u * nwarps) {
+        for (uint32_t w0 = warp << 5; w0 < g.NW; w0 += nwarps << 5) {
+            const uint32_t w = w0 + lane;
+            uint32_t acc_r = 0xFFFFFFFFu, acc = 0;
+            if (w < g.NW) {
+                const uint32_t valid = g.valid(w);
+                uint32_t lead = piece_leaders(t, w, valid);
+                const uint32_t roots = t.ROOT[w];
+                const uint32_t nv = (uint32_t)__popc(valid);
+                while (lead) {
+                    const uint32_t b = __ffs(lead) - 1u;
+                    lead &= lead - 1u;
+                    const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
+                    const uint32_t n = (w << 5) + b;
+                    const bool is_root = (roots >> b) & 1u;
+                    const uint32_t r = is_root ? n : (uint32_t)u16[n];
+                    if (r != acc_r) {
+                        if (acc) add16(u16, acc_r, acc);
+                        acc_r = r;
+                        acc = 0;
+                    }
+                    acc += end - b - ((kMinusOne && is_root) ? 1u : 0u);
+                }
+            }
+            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, acc_r);
+            const uint32_t sum = __reduce_add_sync(grp, acc);
+            if (acc_r != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(grp) - 1) && sum) add16(u16, acc_r, sum);
+        }
+    } else {
+        for (uint32_t w = warp; w < g.NW; w += nwarps) {
+            const uint32_t valid = g.valid(w);
+            const uint32_t lead = piece_leaders(t, w, valid);
+            if ((lead >> lane) & 1u) {
+                const uint32_t n = (w << 5) + lane;
+                const uint32_t next = lead & ~mask_le(lane);
+                const uint32_t end = next ? (uint32_t)(__ffs(next) - 1) : (uint32_t)__popc(valid);
+                const bool is_root = (t.ROOT[w] >> lane) & 1u;
+                const uint32_t r = is_root ? n : (uint32_t)u16[n];
+                add16(u16, r, end - lane - ((kMinusOne && is_root) ? 1u : 0u));
+            }
+        }
+    }
+}
+
 }  // namespace rbim

@@ -398,19 +398,8 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             red.downs_t = d;
         }
     }
-    // Cluster sizes into the root words: one add per run piece (the sites of
-    // a word split into maximal runs share a root), made by its first site.
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t valid = g.valid(w);
-        const uint32_t lead = piece_leaders(t, w, valid);
-        if ((lead >> lane) & 1u) {
-            const uint32_t n = (w << 5) + lane;
-            const uint32_t next = lead & ~mask_le(lane);
-            const uint32_t end = next ? (uint32_t)(__ffs(next) - 1) : (uint32_t)__popc(valid);
-            const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
-            add16(u16, r, end - lane);
-        }
-    }
+    // Cluster sizes into the root words.
+    count_pieces<false>(t, u16, warp, nwarps);
     __syncthreads();
     RBIM_PHASE_MARK(7);
     const uint32_t ncl = red.ncl;
@@ -444,12 +433,21 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         RBIM_PHASE_MARK(8);
         const uint32_t g1 = red.g1;
         int mc = 0;
-        for (uint32_t w = warp; w < g.NW; w += nwarps) {
-            const uint32_t n = (w << 5) + lane;
-            const bool root = (t.ROOT[w] >> lane) & 1u;
-            const bool in = n < g.N && (root ? n == g1 : (uint32_t)u16[n] == g1);
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
-            if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
+        // Two words per iteration keep two load chains in flight.
+        for (uint32_t w0 = warp; w0 < g.NW; w0 += 2u * nwarps) {
+            const uint32_t w1 = w0 + nwarps;
+            const uint32_t n0 = (w0 << 5) + lane, n1 = (w1 << 5) + lane;
+            const uint32_t rt0 = t.ROOT[w0], rt1 = w1 < g.NW ? t.ROOT[w1] : 0u;
+            const bool ok0 = n0 < g.N, ok1 = n1 < g.N;
+            const uint32_t p0 = ok0 ? (uint32_t)u16[n0] : 0u, p1 = ok1 ? (uint32_t)u16[n1] : 0u;
+            const bool in0 = ok0 && (((rt0 >> lane) & 1u) ? n0 == g1 : p0 == g1);
+            const bool in1 = ok1 && (((rt1 >> lane) & 1u) ? n1 == g1 : p1 == g1);
+            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, in0);
+            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, in1);
+            if (lane == 0) {
+                mc += (int)__popc(m0) - 2 * (int)__popc(m0 & t.S[w0]);
+                if (w1 < g.NW) mc += (int)__popc(m1) - 2 * (int)__popc(m1 & t.S[w1]);
+            }
         }
         if (lane == 0) red.mc[warp] = mc;
         __syncthreads();
