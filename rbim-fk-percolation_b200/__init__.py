@@ -15,7 +15,7 @@ itself as ``rbim_b200`` in ``sys.modules``.
 
 import sys as _sys
 
-from . import _native
+from . import _native, autotune
 from ._native import RbimError
 from .clusters import (
     activate_bonds,

@@ -149,12 +149,15 @@ int resident_max_l()
 
 int resident_default_threads(int l_max)
 {
-    // About eight words per warp, as a power of two in [128, 1024].
-    const int nw = (l_max * l_max + 31) / 32;
-    const int want = 32 * ((nw + 7) / 8);
-    int t = 128;
-    while (t < want && t < 1024) t *= 2;
-    return t;
+    // At 64 registers a thread an SM holds 1024 of this kernel's threads
+    // whatever the CTA size, and several small CTAs per SM hide each other's
+    // barrier waits better than one large one; so the CTA is as small as the
+    // lattice allows before its per-thread work grows long.  Measured on
+    // B200: 128 threads up to L = 32, 256 up to 96, 512 up to 128, then 1024.
+    if (l_max <= 32) return 128;
+    if (l_max <= 96) return 256;
+    if (l_max <= 128) return 512;
+    return 1024;
 }
 
 // Shared scratch of one CTA.
@@ -686,8 +689,9 @@ cudaError_t launch_sweeps_lc(const rbim_chain_t *chains, int n_chains, int l_max
     return cudaGetLastError();
 }
 
-// Size classes with a compile-time layout: the default thread counts of
-// 128 < L <= 256 and 64 < L <= 128 (1024 threads) and 32 < L <= 64 (512).
+// Size classes with a compile-time layout, at their default thread counts:
+// 128 < L <= 256 (1024 threads), 96 < L <= 128 (512), 64 < L <= 96 and
+// 32 < L <= 64 (256).
 template <int NT>
 cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                              const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
@@ -696,10 +700,13 @@ cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max
     if (NT == 1024 && l_max > 128 && l_max <= 256)
         return launch_sweeps_lc<NT, 256>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
                                          n_sweeps, grid, queue, status, stream);
-    if (NT == 1024 && l_max > 64 && l_max <= 128)
+    if (NT == 512 && l_max > 96 && l_max <= 128)
         return launch_sweeps_lc<NT, 128>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
                                          n_sweeps, grid, queue, status, stream);
-    if (NT == 512 && l_max > 32 && l_max <= 64)
+    if (NT == 256 && l_max > 64 && l_max <= 96)
+        return launch_sweeps_lc<NT, 96>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                        n_sweeps, grid, queue, status, stream);
+    if (NT == 256 && l_max > 32 && l_max <= 64)
         return launch_sweeps_lc<NT, 64>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
                                         n_sweeps, grid, queue, status, stream);
     return launch_sweeps_lc<NT, 0>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,

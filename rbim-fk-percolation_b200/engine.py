@@ -30,6 +30,12 @@ def _torch():
     return torch
 
 
+def _package():
+    import importlib
+
+    return importlib.import_module(__package__)
+
+
 def require_cuda(device=None):
     """Return the CUDA device to use; raise if there is none (no CPU fallback exists)."""
     torch = _torch()
@@ -224,10 +230,16 @@ class ChainSet:
         engine (one lattice per CTA, one launch per power-of-two size class),
         larger ones up to ``rbim_cluster_max_l()`` on the cluster engine (one
         lattice per thread-block cluster, one launch per cluster size), and
-        any larger still on the plain engine.
+        any larger still on the plain engine.  ``threads`` fixes the resident
+        CTA size; 0 takes the autotuner's choice when it is enabled
+        (``autotune.enable()``), else the library's rule.
         """
+        self._run_batched_fixed(n_sweeps, threads, tuned=threads == 0)
+
+    def _run_batched_fixed(self, n_sweeps: int, threads: int, tuned: bool = False) -> None:
         if n_sweeps <= 0:
             return
+        from . import autotune
         nbytes = int(self.lib.rbim_batched_workspace_bytes())
         ws = self._workspace(nbytes)
         recs = self._ptr(self.records) if self.records is not None else None
@@ -235,9 +247,10 @@ class ChainSet:
             for kind, first, count, l_max in self.buckets:
                 ptr = ctypes.c_void_p(self.chains.data_ptr() + 96 * first)
                 if kind == 0:
+                    nt = autotune.tuned_threads(l_max, self.device) if tuned else threads
                     rc = self.lib.rbim_sweeps_batched(
                         ptr, count, l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
-                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), int(threads),
+                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), int(nt),
                         self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
                     _native.check(rc, "rbim_sweeps_batched")
                 elif kind == 1:

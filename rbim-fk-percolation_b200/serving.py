@@ -33,7 +33,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-from . import _native
+from . import _native, autotune
 from .engine import _torch, require_cuda
 from .packing import pack_couplings, threshold, words_for
 from .simulation import ScanPlan, assemble_scan, plan_temperature_scan
@@ -380,8 +380,9 @@ class ScanServer:
                 l_max = max(a.plan.L for a in group)
                 base = self.desc_dev.data_ptr() + 96 * first
                 if key[0] == 0:
+                    nt = self.threads or autotune.tuned_threads(l_max, self.device)
                     rc = self.lib.rbim_sweeps_batched(ctypes.c_void_p(base), count, l_max, pool, pool, ai, af, None,
-                                                      self.quantum, self.threads, st, qw, self.queue_ws.numel(), sp)
+                                                      self.quantum, nt, st, qw, self.queue_ws.numel(), sp)
                     _native.check(rc, "rbim_sweeps_batched")
                     self.launches += 1
                 elif key[0] == 1:
