@@ -33,6 +33,10 @@ constexpr uint32_t kMaxResidentSites = 65536;  // 16-bit parents
 // kernels' static shared scratch.
 constexpr size_t kMaxSmem = 227 * 1024 - 8 * 1024;
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
+// Shared memory of one SM, and an allowance for a CTA's static shared scratch
+// and the per-CTA reservation, when deciding how many CTAs fit an SM.
+constexpr size_t kSmemPerSm = 228 * 1024;
+constexpr size_t kStaticSmem = 2 * 1024;
 
 __host__ __device__ constexpr size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
@@ -153,10 +157,11 @@ int resident_default_threads(int l_max)
     // whatever the CTA size, and several small CTAs per SM hide each other's
     // barrier waits better than one large one; so the CTA is as small as the
     // lattice allows before its per-thread work grows long.  Measured on
-    // B200: 128 threads up to L = 32, 256 up to 96, 512 up to 128, then 1024.
+    // B200: 128 threads up to L = 32, 256 up to 96, then 512 while two CTAs'
+    // shared memory fits an SM (up to L = 176), then 1024.
     if (l_max <= 32) return 128;
     if (l_max <= 96) return 256;
-    if (l_max <= 128) return 512;
+    if (2 * (resident_layout_c((uint32_t)l_max).bytes + kStaticSmem) <= kSmemPerSm) return 512;
     return 1024;
 }
 
@@ -690,8 +695,8 @@ cudaError_t launch_sweeps_lc(const rbim_chain_t *chains, int n_chains, int l_max
 }
 
 // Size classes with a compile-time layout, at their default thread counts:
-// 128 < L <= 256 (1024 threads), 96 < L <= 128 (512), 64 < L <= 96 and
-// 32 < L <= 64 (256).
+// 128 < L <= 256 (1024 threads), 96 < L <= 128 and 128 < L <= 176 (512),
+// 64 < L <= 96 and 32 < L <= 64 (256).
 template <int NT>
 cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                              const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
@@ -702,6 +707,10 @@ cudaError_t launch_sweeps_nt(const rbim_chain_t *chains, int n_chains, int l_max
                                          n_sweeps, grid, queue, status, stream);
     if (NT == 512 && l_max > 96 && l_max <= 128)
         return launch_sweeps_lc<NT, 128>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                         n_sweeps, grid, queue, status, stream);
+    if (NT == 512 && l_max > 128 && l_max <= 176 &&
+        2 * (resident_layout_c(176).bytes + kStaticSmem) <= kSmemPerSm)
+        return launch_sweeps_lc<NT, 176>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,
                                          n_sweeps, grid, queue, status, stream);
     if (NT == 256 && l_max > 64 && l_max <= 96)
         return launch_sweeps_lc<NT, 96>(chains, n_chains, l_max, spin_pool, coupling_pool, acc_i, acc_f, rec,

@@ -110,7 +110,7 @@ def _chain(rb, orc, Ls, engine, n_therm=5, n_bins=3, spb=7, p=0.1, temps=(1.0, 2
     return cs, specs, J_host
 
 
-@pytest.mark.parametrize("L", [3, 4, 8, 16, 32, 48, 64])
+@pytest.mark.parametrize("L", [3, 4, 8, 16, 32, 48, 64, 80, 100, 150, 180])
 def test_batched_chain_bit_exact(rb, orc, L):
     _chain(rb, orc, [L] * 6, "batched")
 
