@@ -219,19 +219,19 @@ int rbim_cluster_max_l(void)
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
     std::lock_guard<std::mutex> lock(mu);
     if (cached[dev]) return cached[dev] > 0 ? cached[dev] : 0;
-    int ok_c[17] = {};  // per cluster size: 1 schedulable, -1 not
+    int ok_c[17][2] = {};  // per cluster size and CTA size: 1 schedulable, -1 not
     int best = -1;
     for (int L = 1024; L > rbim::resident_max_l(); --L) {
-        const uint32_t C = rbim::cluster_size_for((uint32_t)L);
-        if (C == 0) continue;
-        if (!rbim::cluster_layout_fits(rbim::cluster_layout((uint32_t)L, C))) continue;
-        if (ok_c[C] == 0) {
+        const rbim::ClusterPlan plan = rbim::cluster_plan((uint32_t)L);
+        if (plan.C == 0) continue;
+        const int m = plan.threads == 512u ? 1 : 0;
+        if (ok_c[plan.C][m] == 0) {
             int clusters = 0;
-            const cudaError_t e = rbim::cluster_occupancy((uint32_t)L, C, &clusters);
-            ok_c[C] = (e == cudaSuccess && clusters > 0) ? 1 : -1;
+            const cudaError_t e = rbim::cluster_occupancy((uint32_t)L, &clusters);
+            ok_c[plan.C][m] = (e == cudaSuccess && clusters > 0) ? 1 : -1;
             if (e != cudaSuccess) cudaGetLastError();
         }
-        if (ok_c[C] > 0) {
+        if (ok_c[plan.C][m] > 0) {
             best = L;
             break;
         }

@@ -44,23 +44,20 @@ namespace rbim {
 
 namespace {
 
-constexpr int kCT = 1024;               // threads per CTA
 constexpr uint32_t kTileMax = 65536;    // 16-bit tile parents
+constexpr uint32_t kTileHalf = 32768;   // tiles of the 512-thread mode
 constexpr uint32_t kClusterMax = 16;    // non-portable cluster size limit
-constexpr uint32_t kSlotsPerThread = 4; // hash size <= 4 * kCT
+constexpr uint32_t kHashMax = 4096;     // node slots per tile (12 bits of a node id)
+constexpr uint32_t kHalfTilesMax = 5;   // most tiles per lattice in the 512-thread mode
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
-constexpr size_t kSmemBudget = 227 * 1024 - 4 * 1024;
+constexpr size_t kSmemBudget = 227 * 1024 - 4 * 1024;  // one CTA per SM
+constexpr size_t kSmemPerSm = 228 * 1024;
+constexpr size_t kStaticSmem = 2 * 1024;
 
 __host__ __device__ constexpr size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
 
 }  // namespace
 
-uint32_t cluster_size_for(uint32_t L)
-{
-    for (uint32_t C = 2; C <= kClusterMax; ++C)
-        if (cluster_tiles_ok(L, C)) return C;
-    return 0;
-}
 
 namespace {
 
@@ -71,7 +68,7 @@ __host__ __device__ constexpr uint32_t cluster_hash_size(uint32_t l_max, uint32_
     const uint32_t rows = T / l_max + 2u;
     const uint32_t bound = 2u * l_max + 2u * rows + 1u;
     uint32_t h = 64;
-    while (h < bound + bound / 2u) h *= 2;
+    while (h < bound + bound / 4u) h *= 2;
     return h;
 }
 
@@ -114,10 +111,31 @@ __host__ __device__ constexpr ClusterLayout cluster_layout_c(uint32_t l_max, uin
 
 ClusterLayout cluster_layout(uint32_t l_max, uint32_t C) { return cluster_layout_c(l_max, C); }
 
-bool cluster_layout_fits(const ClusterLayout &ly)
+bool cluster_layout_fits(const ClusterLayout &ly, uint32_t threads)
 {
-    return ly.bytes <= kSmemBudget && ly.hs <= kSlotsPerThread * kCT && ly.t_max <= kTileMax;
+    if (ly.hs > kHashMax) return false;
+    if (threads == 512u) return ly.t_max <= kTileHalf && 2 * (ly.bytes + kStaticSmem) <= kSmemPerSm;
+    return ly.bytes <= kSmemBudget && ly.t_max <= kTileMax;
 }
+
+ClusterPlan cluster_plan(uint32_t L)
+{
+    // Two 512-thread CTAs per SM hide each other's barrier waits better than
+    // one of 1024 (as in the resident engine), but twice the tiles also mean
+    // twice the boundary bonds and wider cluster barriers: on B200 the
+    // smaller tiles win up to 5 per lattice (L = 300: +10 %, L = 384: +6 %)
+    // and lose at 8 (L = 512) and 16 (L = 724).
+    for (uint32_t C = 2; C <= kHalfTilesMax; ++C) {
+        if (!cluster_tiles_ok(L, C, kTileHalf)) continue;
+        if (cluster_layout_fits(cluster_layout(L, C), 512u)) return {C, 512u};
+        break;
+    }
+    for (uint32_t C = 2; C <= kClusterMax; ++C)
+        if (cluster_tiles_ok(L, C) && cluster_layout_fits(cluster_layout(L, C), 1024u)) return {C, 1024u};
+    return {0u, 0u};
+}
+
+uint32_t cluster_size_for(uint32_t L) { return cluster_plan(L).C; }
 
 namespace {
 
@@ -218,6 +236,7 @@ __device__ __forceinline__ uint32_t tile_ynext(const uint32_t *S, uint32_t w, ui
 // the same Philox word as in the whole-lattice engines.  OV keeps the y-bonds
 // inside the tile; y-seam bonds go to YS (bit = row - x0), the y-bond from
 // the tile's last site into the next tile to red.tile_end.
+template <int NT>
 __device__ __forceinline__ void tile_activate(const Ctx &x, const Tile &tl, const SweepRng &rng, const uint32_t *gJH,
                                               const uint32_t *gJV, uint32_t front, CRed &red, uint32_t warp,
                                               uint32_t nwarps, uint32_t tid)
@@ -299,7 +318,7 @@ __device__ __forceinline__ void tile_activate(const Ctx &x, const Tile &tl, cons
     }
     // Flip bits: Philox block q of stream 1 covers global words 4q .. 4q+3.
     const uint32_t nblk = (g.NW + 3u) >> 2;
-    for (uint32_t q = tid; q < nblk; q += kCT) {
+    for (uint32_t q = tid; q < nblk; q += NT) {
         const U4 rr = philox_block(rng.key, chunk0 + q, rng.sweep, kStreamFlip);
         const uint32_t w = 4u * q;
         t.FLIP[w] = rr.x;
@@ -335,7 +354,8 @@ struct Dist {
     }
     __device__ __forceinline__ uint32_t key(uint32_t node) const
     {
-        return ((node >> 16) << 16) | *((volatile uint32_t *)(cl.map_shared_rank(HK, node >> 16) + (node & 0xFFFFu)));
+        return ((node >> 16) << 16) |
+               (*((volatile uint32_t *)(cl.map_shared_rank(HK, node >> 16) + (node & 0xFFFFu))) & 0xFFFFu);
     }
     __device__ __forceinline__ unsigned long long ld(uint32_t node) const
     {
@@ -436,6 +456,7 @@ struct Dist {
 // (b) Boundary bonds owned by this tile: x-bonds of its last L sites, the
 // y-bond from its last site into the next tile, and the y-seam bonds of the
 // rows ending in it.
+template <int NT>
 __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, const Dist &d, uint32_t tile_end,
                                               uint32_t tid)
 {
@@ -444,7 +465,7 @@ __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, cons
     const uint32_t n_rows = rows_end - tl.x0;
     const uint32_t items = tl.L + 1u + n_rows;
     const uint32_t nxt = tl.c + 1u == tl.C ? 0u : tl.c + 1u;
-    for (uint32_t i = tid; i < items; i += kCT) {
+    for (uint32_t i = tid; i < items; i += NT) {
         uint32_t a, tb, bl;
         int ex = 0, ey = 0;
         if (i < tl.L) {
@@ -491,6 +512,7 @@ __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, cons
 // Spin halo after a flip: the first L spins of the next tile (of the first
 // tile, for the last one) at bits Tc .. Tc+L-1, and the front spin (the row
 // start of the tile's first row, when that row began in the previous tile).
+template <int NT>
 __device__ __forceinline__ void tile_halo(const Ctx &x, const Tile &tl, const cg::cluster_group &cl, CRed &red,
                                           uint32_t tid)
 {
@@ -500,7 +522,7 @@ __device__ __forceinline__ void tile_halo(const Ctx &x, const Tile &tl, const cg
     const uint32_t lw = (tl.L + 31u) >> 5;
     const uint32_t sh = tl.Tc & 31u, d0 = tl.Tc >> 5;
     const uint32_t lmask = (tl.L & 31u) ? (1u << (tl.L & 31u)) - 1u : 0xFFFFFFFFu;
-    for (uint32_t k = tid; k <= lw; k += kCT) {
+    for (uint32_t k = tid; k <= lw; k += NT) {
         const uint32_t hk = k < lw ? (rs[k] & (k + 1u == lw ? lmask : 0xFFFFFFFFu)) : 0u;
         uint32_t v;
         if (sh == 0u) {
@@ -523,11 +545,12 @@ __device__ __forceinline__ void tile_halo(const Ctx &x, const Tile &tl, const cg
     }
 }
 
+template <int NT>
 __device__ __forceinline__ void tile_energy(const Ctx &x, const Tile &tl, const uint32_t *gJH, const uint32_t *gJV,
                                             uint32_t front, uint32_t tid, uint32_t &unsat, uint32_t &downs)
 {
     const Lat<Word16> &t = x.t;
-    for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+    for (uint32_t w = tid; w < t.g.NW; w += NT) {
         const uint32_t v = t.g.valid(w);
         const uint32_t s = t.S[w];
         const uint32_t re = tile_row_end(tl, w, v);
@@ -544,17 +567,23 @@ __device__ __forceinline__ uint32_t node_root(const Ctx &x, uint32_t k)
     return *((volatile uint32_t *)(x.HW + k));
 }
 
+// Tile root of the node in slot k: the low half of its hash word (the high
+// half carries its root node between the two halves of the propagation).
+__device__ __forceinline__ uint32_t node_key(uint32_t hk) { return hk & 0xFFFFu; }
+
 // The open-tile union and root walks as separate (non-inlined) functions: the
 // cluster kernel keeps more state live across its phases than the resident
 // one, and compiled inline these pointer-chasing loops lose registers to it.
+template <int NT>
 static __device__ __noinline__ void cluster_union(const Lat<Word16> &t, uint32_t tid)
 {
-    phase_union_open(t, tid, kCT);
+    phase_union_open(t, tid, NT);
 }
 
+template <int NT>
 static __device__ __noinline__ void cluster_roots(const Lat<Word16> &t, uint32_t tid)
 {
-    (void)phase_roots_flat(t, tid, kCT);
+    (void)phase_roots_flat(t, tid, NT);
 }
 
 __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g)
@@ -562,10 +591,11 @@ __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g
     return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
 }
 
-// LC > 0: the layout is cluster_layout_c(LC, CC), a compile-time constant,
-// and the cluster has CC CTAs; LC == 0: the layout passed in.
-template <int LC, int CC>
-__global__ void __launch_bounds__(kCT, 1)
+// NT threads per CTA.  LC > 0: the layout is cluster_layout_c(LC, CC), a
+// compile-time constant, and the cluster has CC CTAs; LC == 0: the layout
+// passed in.
+template <int NT, int LC, int CC>
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
     k_cluster_sweeps(rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, const uint32_t *coupling_pool,
                      long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *queue, int *status,
                      ClusterLayout ly_arg)
@@ -576,7 +606,8 @@ __global__ void __launch_bounds__(kCT, 1)
     const ClusterLayout ly = LC > 0 ? kly : ly_arg;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    constexpr uint32_t nwarps = kCT / 32;
+    constexpr uint32_t nwarps = NT / 32;
+    constexpr uint32_t kCap = NT >= 1024 ? kTileMax : kTileHalf;
     const uint32_t C = CC > 0 ? (uint32_t)CC : cl.num_blocks(), c = cl.block_rank();
 
     if (tid == 0) red.err = 0;
@@ -594,7 +625,7 @@ __global__ void __launch_bounds__(kCT, 1)
         __syncthreads();
         const rbim_chain_t &ch = red.ch;
         const bool bad = ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 ||
-                         ch.n_therm < 0 || !cluster_tiles_ok((uint32_t)ch.L, C) ||
+                         ch.n_therm < 0 || !cluster_tiles_ok((uint32_t)ch.L, C, kCap) ||
                          cluster_tile_size((uint32_t)(ch.L * ch.L), C) > ly.t_max;
         if (bad) {
             if (tid == 0 && c == 0) atomicOr(status, kErrBadChain);
@@ -621,12 +652,12 @@ __global__ void __launch_bounds__(kCT, 1)
         const uint32_t s_words = ly.tw + (ly.l_max + 31u) / 32u + 4u;
 
         // Load the tile's spins; zero the halo and padding.
-        for (uint32_t w = tid; w < s_words; w += kCT) t.S[w] = w < tl.tw ? gS[w] & t.g.valid(w) : 0u;
+        for (uint32_t w = tid; w < s_words; w += NT) t.S[w] = w < tl.tw ? gS[w] & t.g.valid(w) : 0u;
         const uint64_t t_end = (uint64_t)ch.n_therm + (uint64_t)ch.n_bins * (uint64_t)ch.sweeps_per_bin;
         uint64_t sweep = ch.sweep;
         const uint64_t stop = min(t_end, sweep + (uint64_t)max(n_sweeps, 0));
         cl.sync();
-        tile_halo(x, tl, cl, red, tid);
+        tile_halo<NT>(x, tl, cl, red, tid);
         __syncthreads();
 
         for (; sweep < stop; ++sweep) {
@@ -636,51 +667,48 @@ __global__ void __launch_bounds__(kCT, 1)
                 red.wrap = 0;
                 red.tile_end = 0;
             }
-            for (uint32_t i = tid; i < 16u; i += kCT) x.YS[i] = 0u;
+            for (uint32_t i = tid; i < 16u; i += NT) x.YS[i] = 0u;
             __syncthreads();
-            tile_activate(x, tl, make_rng(ch.key, sweep, ch.thr), gJH, gJV, front, red, warp, nwarps, tid);
+            tile_activate<NT>(x, tl, make_rng(ch.key, sweep, ch.thr), gJH, gJV, front, red, warp, nwarps, tid);
             __syncthreads();
             phase_heads<Word16>(t, warp, nwarps);
-            for (uint32_t w = tid; w < t.g.NW; w += kCT) t.ROOT[w] = 0u;
-            for (uint32_t k = tid; k < x.hs; k += kCT) {
+            for (uint32_t w = tid; w < t.g.NW; w += NT) t.ROOT[w] = 0u;
+            for (uint32_t k = tid; k < x.hs; k += NT) {
                 x.HK[k] = kEmptyKey;
                 x.HW[k] = Word64::make((c << 16) | k, 0, 0);
             }
             __syncthreads();
-            cluster_union(t, tid);
+            cluster_union<NT>(t, tid);
             __syncthreads();
-            cluster_roots(t, tid);
+            cluster_roots<NT>(t, tid);
             __syncthreads();
             cl.sync();  // every tile's roots are final
 
-            tile_boundary(x, tl, d, red.tile_end, tid);
+            tile_boundary<NT>(x, tl, d, red.tile_end, tid);
             cl.sync();  // every boundary union is done
 
-            // Root node of each of this tile's nodes, and the flip bit of its
-            // cluster (the raw bit of the root node's site).
-            uint32_t rn[kSlotsPerThread], fb[kSlotsPerThread];
-#pragma unroll
-            for (uint32_t j = 0; j < kSlotsPerThread; ++j) {
-                const uint32_t k = tid + j * kCT;
-                rn[j] = kEmptyKey;
-                fb[j] = 0;
-                if (k < x.hs && x.HK[k] != kEmptyKey) {
-                    const uint32_t r = d.root_ro((c << 16) | k);
-                    rn[j] = r;
-                    const uint32_t m = *cl.map_shared_rank(x.HK + (r & 0xFFFFu), r >> 16);
-                    const uint32_t *fl = cl.map_shared_rank(t.FLIP, r >> 16);
-                    fb[j] = (fl[m >> 5] >> (m & 31u)) & 1u;
-                }
+            // Root node of each of this tile's nodes, kept in the high half of
+            // its hash word (tile in 4 bits, slot in 12) until every walk is done.
+            for (uint32_t k = tid; k < x.hs; k += NT) {
+                const uint32_t hk = x.HK[k];
+                if (hk == kEmptyKey) continue;
+                const uint32_t r = d.root_ro((c << 16) | k);
+                x.HK[k] = node_key(hk) | (((r >> 16) << 12 | (r & 0xFFFu)) << 16);
             }
             cl.sync();  // all walks done before the words change
-#pragma unroll
-            for (uint32_t j = 0; j < kSlotsPerThread; ++j) {
-                const uint32_t k = tid + j * kCT;
-                if (rn[j] == kEmptyKey) continue;
-                x.HW[k] = (unsigned long long)rn[j];  // root node | merged size (0)
-                if (rn[j] != ((c << 16) | k)) {
-                    const uint32_t m = x.HK[k];
-                    if (fb[j])
+            // Union-find word -> root node (merged size 0); a merged tile root
+            // takes the flip bit of its cluster: the raw bit of the root
+            // node's site, which no CTA changes.
+            for (uint32_t k = tid; k < x.hs; k += NT) {
+                const uint32_t hk = x.HK[k];
+                if (hk == kEmptyKey) continue;
+                const uint32_t r = ((hk >> 28) << 16) | ((hk >> 16) & 0xFFFu), m = node_key(hk);
+                x.HK[k] = m;
+                x.HW[k] = (unsigned long long)r;
+                if (r != ((c << 16) | k)) {
+                    const uint32_t mr = node_key(*cl.map_shared_rank(x.HK + (r & 0xFFFFu), r >> 16));
+                    const uint32_t *fl = cl.map_shared_rank(t.FLIP, r >> 16);
+                    if ((fl[mr >> 5] >> (mr & 31u)) & 1u)
                         atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
                     else
                         atomicAnd(t.FLIP + (m >> 5), ~(1u << (m & 31u)));
@@ -690,7 +718,7 @@ __global__ void __launch_bounds__(kCT, 1)
             phase_sites<Word16>(t, warp, nwarps, true, false);
             __syncthreads();
             cl.sync();  // every flip is done
-            tile_halo(x, tl, cl, red, tid);
+            tile_halo<NT>(x, tl, cl, red, tid);
             __syncthreads();
 
             if (!measure) continue;
@@ -698,8 +726,8 @@ __global__ void __launch_bounds__(kCT, 1)
             // ---- measurement (reference sw_sweep, src/rbim/swendsen_wang.py:146-172)
             unsigned short *u16 = t.uf.w;
             uint32_t unsat = 0, downs = 0;
-            tile_energy(x, tl, gJH, gJV, red.front, tid, unsat, downs);
-            for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+            tile_energy<NT>(x, tl, gJH, gJV, red.front, tid, unsat, downs);
+            for (uint32_t w = tid; w < t.g.NW; w += NT) {
                 uint32_t roots = t.ROOT[w];
                 while (roots) {
                     const uint32_t bb = __ffs(roots) - 1u;
@@ -713,11 +741,11 @@ __global__ void __launch_bounds__(kCT, 1)
             count_pieces<true>(t, u16, warp, nwarps);
             __syncthreads();
             // OV (no longer needed this sweep) becomes the plane of node marks.
-            for (uint32_t w = tid; w < t.g.NW; w += kCT) t.OV[w] = 0u;
+            for (uint32_t w = tid; w < t.g.NW; w += NT) t.OV[w] = 0u;
             __syncthreads();
             // Merged sizes into the root nodes; mark this tile's nodes in OV.
             uint32_t rootnodes = 0;
-            for (uint32_t k = tid; k < x.hs; k += kCT) {
+            for (uint32_t k = tid; k < x.hs; k += NT) {
                 const uint32_t m = x.HK[k];
                 if (m == kEmptyKey) continue;
                 const uint32_t r = node_root(x, k);
@@ -728,12 +756,12 @@ __global__ void __launch_bounds__(kCT, 1)
             }
             __syncthreads();
             uint32_t nloc = rootnodes;
-            for (uint32_t w = tid; w < t.g.NW; w += kCT) nloc += __popc(t.ROOT[w] & ~t.OV[w]);
+            for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~t.OV[w]);
             cl.sync();  // merged sizes are complete
 
             // Local top two: tile-only clusters and this tile's root nodes.
             unsigned long long k1 = 0, k2 = 0;
-            for (uint32_t w = tid; w < t.g.NW; w += kCT) {
+            for (uint32_t w = tid; w < t.g.NW; w += NT) {
                 uint32_t roots = t.ROOT[w] & ~t.OV[w];
                 while (roots) {
                     const uint32_t bb = __ffs(roots) - 1u;
@@ -742,7 +770,7 @@ __global__ void __launch_bounds__(kCT, 1)
                     top2_merge(k1, k2, size_key((uint32_t)u16[m] + 1u, tl.b + m), 0ull);
                 }
             }
-            for (uint32_t k = tid; k < x.hs; k += kCT) {
+            for (uint32_t k = tid; k < x.hs; k += NT) {
                 if (x.HK[k] == kEmptyKey || node_root(x, k) != ((c << 16) | k)) continue;
                 top2_merge(k1, k2, size_key((uint32_t)(x.HW[k] >> 32), tl.b + x.HK[k]), 0ull);
             }
@@ -762,9 +790,11 @@ __global__ void __launch_bounds__(kCT, 1)
             }
             __syncthreads();
             if (warp == 0) {
-                unsigned long long a1 = red.k1[lane], a2 = red.k2[lane];
+                const bool live = lane < nwarps;
+                unsigned long long a1 = live ? red.k1[lane] : 0ull, a2 = live ? red.k2[lane] : 0ull;
                 warp_top2(a1, a2);
-                uint32_t su = red.unsat[lane], sd = red.downs[lane], sn = red.ncl[lane];
+                uint32_t su = live ? red.unsat[lane] : 0u, sd = live ? red.downs[lane] : 0u;
+                uint32_t sn = live ? red.ncl[lane] : 0u;
                 for (int o = 16; o > 0; o >>= 1) {
                     su += __shfl_xor_sync(0xFFFFFFFFu, su, o);
                     sd += __shfl_xor_sync(0xFFFFFFFFu, sd, o);
@@ -824,13 +854,13 @@ __global__ void __launch_bounds__(kCT, 1)
             const bool many = red.ncl_total > 1u;
             if (many) {
                 // Tile roots of the largest cluster, marked in OH.
-                for (uint32_t w = tid; w < t.g.NW; w += kCT) t.OH[w] = 0u;
+                for (uint32_t w = tid; w < t.g.NW; w += NT) t.OH[w] = 0u;
                 __syncthreads();
                 if (tid == 0 && g1 >= tl.b && g1 < tl.b + tl.Tc) {
                     const uint32_t m = g1 - tl.b;
                     atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
                 }
-                for (uint32_t k = tid; k < x.hs; k += kCT) {
+                for (uint32_t k = tid; k < x.hs; k += NT) {
                     if (x.HK[k] == kEmptyKey) continue;
                     const uint32_t r = node_root(x, k);
                     const uint32_t rt = r >> 16;
@@ -891,7 +921,7 @@ __global__ void __launch_bounds__(kCT, 1)
                               acc_f + (ch.acc_off + red.cur_bin) * kAccF64);
             chains[item].sweep = stop;
         }
-        for (uint32_t w = tid; w < tl.tw; w += kCT) gS[w] = t.S[w] & t.g.valid(w);
+        for (uint32_t w = tid; w < tl.tw; w += NT) gS[w] = t.S[w] & t.g.valid(w);
         cl.sync();  // halo reads of this chain are over before the next load
     }
     if (tid == 0 && red.err) atomicOr(status, red.err);
@@ -901,14 +931,14 @@ __global__ void __launch_bounds__(kCT, 1)
 
 namespace {
 
-template <int LC, int CC>
+template <int NT, int LC, int CC>
 cudaError_t occupancy_t(const ClusterLayout &ly, uint32_t C, int *clusters)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_cluster_sweeps<LC, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_cluster_sweeps<NT, LC, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ly.bytes);
     if (e != cudaSuccess) return e;
     if (C > 8u) {
-        e = cudaFuncSetAttribute(k_cluster_sweeps<LC, CC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        e = cudaFuncSetAttribute(k_cluster_sweeps<NT, LC, CC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
     }
     cudaLaunchConfig_t cfg = {};
@@ -918,20 +948,20 @@ cudaError_t occupancy_t(const ClusterLayout &ly, uint32_t C, int *clusters)
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3(C, 1, 1);
-    cfg.blockDim = dim3(kCT, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = ly.bytes;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(clusters, k_cluster_sweeps<LC, CC>, &cfg);
+    return cudaOccupancyMaxActiveClusters(clusters, k_cluster_sweeps<NT, LC, CC>, &cfg);
 }
 
-template <int LC, int CC>
+template <int NT, int LC, int CC>
 cudaError_t launch_t(const ClusterLayout &ly, uint32_t C, const rbim_chain_t *chains, int n_chains,
                      uint32_t *spin_pool, const uint32_t *coupling_pool, long long *acc_i, double *acc_f,
                      int32_t *rec, int n_sweeps, int *queue, int *status, cudaStream_t stream)
 {
     int clusters = 0;
-    cudaError_t e = occupancy_t<LC, CC>(ly, C, &clusters);
+    cudaError_t e = occupancy_t<NT, LC, CC>(ly, C, &clusters);
     if (e != cudaSuccess) return e;
     if (clusters <= 0) return cudaErrorInvalidConfiguration;
     const int n_clusters = std::min(clusters, n_chains);
@@ -944,56 +974,72 @@ cudaError_t launch_t(const ClusterLayout &ly, uint32_t C, const rbim_chain_t *ch
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3((unsigned)n_clusters * C, 1, 1);
-    cfg.blockDim = dim3(kCT, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = ly.bytes;
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_cluster_sweeps<LC, CC>, const_cast<rbim_chain_t *>(chains), n_chains, spin_pool,
-                           coupling_pool, acc_i, acc_f, rec, n_sweeps, queue, status, ly);
+    e = cudaLaunchKernelEx(&cfg, k_cluster_sweeps<NT, LC, CC>, const_cast<rbim_chain_t *>(chains), n_chains,
+                           spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps, queue, status, ly);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
-// The classes with a compile-time layout: 4-CTA clusters up to L = 512 and
-// 16-CTA clusters up to L = 1024 (the largest lattices of those sizes).
-int layout_class(uint32_t l_max, uint32_t C)
+// One launch configuration: CTA size, compile-time layout class and cluster
+// size, and the layout.  The classes with a compile-time layout are the two
+// benchmark sizes: L = 512 (4 CTAs) and L = 1024 (16 CTAs), both with 1024
+// threads; each covers the smaller lattices of the same plan.
+struct Launch {
+    uint32_t threads, lc, C;
+    ClusterLayout ly;
+};
+
+Launch launch_for(uint32_t l_max)
 {
-    if (C == 4u && l_max <= 512u && cluster_size_for(512u) == 4u) return 512;
-    if (C == 16u && l_max <= 1024u && cluster_size_for(1024u) == 16u) return 1024;
-    return 0;
+    const ClusterPlan plan = cluster_plan(l_max);
+    Launch l{plan.threads, 0u, plan.C, {}};
+    if (plan.C == 0) return l;
+    const ClusterPlan p512 = cluster_plan(512u), p1024 = cluster_plan(1024u);
+    if (plan.threads == p512.threads && plan.C == p512.C && l_max <= 512u && p512.threads == 1024u && p512.C == 4u)
+        l.lc = 512u;
+    else if (plan.threads == p1024.threads && plan.C == p1024.C && l_max <= 1024u && p1024.threads == 1024u &&
+             p1024.C == 16u)
+        l.lc = 1024u;
+    l.ly = cluster_layout(l.lc ? l.lc : l_max, plan.C);
+    return l;
 }
 
 }  // namespace
 
-cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters)
+cudaError_t cluster_occupancy(uint32_t l_max, int *clusters)
 {
     *clusters = 0;
-    const int lc = layout_class(l_max, C);
-    const ClusterLayout ly = lc ? cluster_layout((uint32_t)lc, C) : cluster_layout(l_max, C);
-    if (!cluster_layout_fits(ly)) return cudaSuccess;
-    if (lc == 512) return occupancy_t<512, 4>(ly, C, clusters);
-    if (lc == 1024) return occupancy_t<1024, 16>(ly, C, clusters);
-    return occupancy_t<0, 0>(ly, C, clusters);
+    const Launch l = launch_for(l_max);
+    if (l.C == 0 || !cluster_layout_fits(l.ly, l.threads)) return cudaSuccess;
+    if (l.lc == 512) return occupancy_t<1024, 512, 4>(l.ly, l.C, clusters);
+    if (l.lc == 1024) return occupancy_t<1024, 1024, 16>(l.ly, l.C, clusters);
+    if (l.threads == 512) return occupancy_t<512, 0, 0>(l.ly, l.C, clusters);
+    return occupancy_t<1024, 0, 0>(l.ly, l.C, clusters);
 }
 
 cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                                   const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
                                   int n_sweeps, int *queue, int *status, cudaStream_t stream)
 {
-    const uint32_t C = cluster_size_for((uint32_t)l_max);
-    if (C == 0) return cudaErrorInvalidValue;
-    const int lc = layout_class((uint32_t)l_max, C);
-    const ClusterLayout ly = lc ? cluster_layout((uint32_t)lc, C) : cluster_layout((uint32_t)l_max, C);
-    if (!cluster_layout_fits(ly)) return cudaErrorInvalidConfiguration;
-    if (lc == 512)
-        return launch_t<512, 4>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
+    const Launch l = launch_for((uint32_t)l_max);
+    if (l.C == 0) return cudaErrorInvalidValue;
+    if (!cluster_layout_fits(l.ly, l.threads)) return cudaErrorInvalidConfiguration;
+    if (l.lc == 512)
+        return launch_t<1024, 512, 4>(l.ly, l.C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                      n_sweeps, queue, status, stream);
+    if (l.lc == 1024)
+        return launch_t<1024, 1024, 16>(l.ly, l.C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                        n_sweeps, queue, status, stream);
+    if (l.threads == 512)
+        return launch_t<512, 0, 0>(l.ly, l.C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec,
+                                   n_sweeps, queue, status, stream);
+    return launch_t<1024, 0, 0>(l.ly, l.C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
                                 queue, status, stream);
-    if (lc == 1024)
-        return launch_t<1024, 16>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps,
-                                  queue, status, stream);
-    return launch_t<0, 0>(ly, C, chains, n_chains, spin_pool, coupling_pool, acc_i, acc_f, rec, n_sweeps, queue,
-                          status, stream);
 }
 
 }  // namespace rbim

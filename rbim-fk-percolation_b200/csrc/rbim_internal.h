@@ -53,19 +53,27 @@ __host__ __device__ constexpr uint32_t cluster_tile_size(uint32_t N, uint32_t C)
     return (t + 127u) & ~127u;
 }
 
-// C tiles fit an L x L lattice when every tile holds between L and 65536 sites.
-__host__ __device__ constexpr bool cluster_tiles_ok(uint32_t L, uint32_t C)
+// C tiles fit an L x L lattice when every tile holds between L and `cap`
+// sites.
+__host__ __device__ constexpr bool cluster_tiles_ok(uint32_t L, uint32_t C, uint32_t cap = 65536u)
 {
     const uint32_t N = L * L, T = cluster_tile_size(N, C);
-    if (T > 65536u || T < L) return false;
+    if (T > cap || T < L) return false;
     const uint32_t before = (C - 1u) * T;
     return before < N && N - before >= L;
 }
 
+// How a lattice of size L runs on the cluster engine: C CTAs of `threads`
+// threads (1024 with tiles of up to 65536 sites, one CTA per SM; 512 with
+// tiles of up to 32768 sites, two CTAs per SM).  C == 0: it does not.
+struct ClusterPlan {
+    uint32_t C, threads;
+};
+ClusterPlan cluster_plan(uint32_t L);
 uint32_t cluster_size_for(uint32_t L);
 ClusterLayout cluster_layout(uint32_t l_max, uint32_t C);
-bool cluster_layout_fits(const ClusterLayout &ly);
-cudaError_t cluster_occupancy(uint32_t l_max, uint32_t C, int *clusters);
+bool cluster_layout_fits(const ClusterLayout &ly, uint32_t threads);
+cudaError_t cluster_occupancy(uint32_t l_max, int *clusters);
 cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                                   const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
                                   int n_sweeps, int *queue, int *status, cudaStream_t stream);
