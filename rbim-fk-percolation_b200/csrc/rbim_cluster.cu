@@ -155,6 +155,7 @@ struct CRed {
     uint32_t front, tile_end;
     Acc acc;
     long long cur_bin;
+    long long rec[kRecLen];
     rbim_chain_t ch;
 };
 
@@ -810,7 +811,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 }
             }
             cl.sync();  // partials are visible
-            long long rec[kRecLen];
+            long long *rec = red.rec;  // rank 0's record of the sweep
             if (c == 0 && warp == 0) {
                 unsigned long long a1 = 0, a2 = 0;
                 uint32_t su = 0, sd = 0, sn = 0;
