@@ -101,34 +101,34 @@ __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const Swe
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint32_t c = c0 + k * nwarps;
-            uint32_t dh[4], dv[4];
-            bool refine = false;
+            // Acceptance of this lane's eight draws, before the satisfied
+            // masks: bit 0 horizontal (low half), bit 16 vertical (high half).
+            uint32_t acc[4], eq = 0;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 const uint32_t w = u4_word(r[k], s);
-                const uint32_t bh = (__shfl_sync(0xFFFFFFFFu, sh[k], s) >> lane) & 1u;
-                const uint32_t bv = (__shfl_sync(0xFFFFFFFFu, sv[k], s) >> lane) & 1u;
-                dh[s] = bh ? bond_decide(rng, w & 0xFFFFu) : 0u;
-                dv[s] = bv ? bond_decide(rng, w >> 16) : 0u;
-                refine |= (dh[s] == 2u) | (dv[s] == 2u);
+                const uint32_t lo = w & 0xFFFFu, hi = w >> 16;
+                acc[s] = ((rng.thr_all || lo < rng.thr_hi) ? 1u : 0u) | ((rng.thr_all || hi < rng.thr_hi) ? 0x10000u : 0u);
+                eq |= ((lo == rng.thr_hi) ? 1u : 0u) << (2 * s);
+                eq |= ((hi == rng.thr_hi) ? 2u : 0u) << (2 * s);
             }
-            if (refine) {
+            if (!rng.thr_all && __any_sync(0xFFFFFFFFu, eq != 0u)) {
                 const U4 q = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBondLow);
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const uint32_t w = u4_word(q, s);
-                    if (dh[s] == 2u) dh[s] = (w & 0xFFFFu) < rng.thr_lo ? 1u : 0u;
-                    if (dv[s] == 2u) dv[s] = (w >> 16) < rng.thr_lo ? 1u : 0u;
+                    if ((eq >> (2 * s)) & 1u) acc[s] |= ((w & 0xFFFFu) < rng.thr_lo) ? 1u : 0u;
+                    if ((eq >> (2 * s)) & 2u) acc[s] |= ((w >> 16) < rng.thr_lo) ? 0x10000u : 0u;
                 }
             }
             uint32_t oh = 0, ov = 0;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, dh[s] != 0u);
-                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, dv[s] != 0u);
+                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, acc[s] & 1u);
+                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, acc[s] >> 16);
                 if (lane == (uint32_t)s) {
-                    oh = bh;
-                    ov = bv;
+                    oh = bh & sh[k];
+                    ov = bv & sv[k];
                 }
             }
             if (lane < 4u && wq[k] < g.NW) {
