@@ -277,6 +277,35 @@ def config_lines(rb, dev, seed):
     return out
 
 
+def c4_full_line(rb, dev, seed, sweeps=2):
+    """The whole uneven-size configuration in one ChainSet: L in {32, 48, 64, 96, 128, 192, 256, 512},
+    p in {0.02, 0.05, 0.08, 0.10}, 4096 (32/L)^2 realizations (rounded up to 8) x 32 temperatures per (L, p);
+    one run_batched call advances every lattice (one launch per size bucket)."""
+    import torch
+
+    temps = np.linspace(1.2, 2.4, 32)
+    ps = [0.02, 0.05, 0.08, 0.10]
+    t0 = time.perf_counter()
+    specs, couplings = [], []
+    for L in (32, 48, 64, 96, 128, 192, 256, 512):
+        n_real = int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
+        sp, cp = build_chains(rb, L, ps, n_real, temps, seed + L, 1000)
+        base = len(couplings)
+        for s_ in sp:
+            s_.realization += base
+        specs += sp
+        couplings += cp
+    cs = rb.ChainSet(specs, couplings, device=dev)
+    cs.init_spins(hot=True)
+    setup = time.perf_counter() - t0
+    sites = float(sum(s_.L * s_.L for s_ in specs))
+    cs.run_batched(1)
+    t = time_sweeps(cs, sweeps)
+    return {"lattices": len(specs), "sites": sites, "sweeps": sweeps, "ms_per_sweep_of_all": 1e3 * t / sweeps,
+            "lattice_sweeps_per_s": len(specs) * sweeps / t, "site_updates_per_s": sites * sweeps / t,
+            "host_setup_s": setup, "launches_per_sweep": len(cs.buckets)}
+
+
 def serving_leg(rb, dev, seconds, rate, scale, seed, quantum):
     """Poisson stream of temperature-scan requests (the serving configuration's distribution of L, p,
     temperatures and realizations, sweeps scaled by `scale`) through the continuous-batching server."""
@@ -357,6 +386,8 @@ def main():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--chains", type=int, default=0, help="use only the first N chains (profiling runs)")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' lines")
+    ap.add_argument("--c4-full", action="store_true",
+                    help="also time the whole uneven-size configuration (about 1e6 lattices; slow host setup)")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="serving leg arrival window (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-scale", type=float, default=0.004, help="sweeps per request scaled by this factor")
@@ -490,6 +521,8 @@ def main():
     configs = None
     if rank == 0 and not args.no_configs:
         configs = config_lines(rb, dev, args.seed)
+    if rank == 0 and args.c4_full:
+        configs = dict(configs or {}, c4_full=c4_full_line(rb, dev, args.seed))
     serving = None
     if rank == 0 and args.serve_seconds > 0:
         serving = serving_leg(rb, dev, args.serve_seconds, args.serve_rate, args.serve_scale, args.seed,

@@ -111,6 +111,11 @@ int64_t rbim_plane_words(int64_t L);
 /* Largest L the resident (on-chip) engine accepts. */
 int rbim_resident_max_l(void);
 
+/* CTA size (threads) the resident engine uses for lattices of up to L x L
+ * sites when rbim_sweeps_batched is called with threads = 0 (0 if L is out of
+ * range): small CTAs while several fit an SM. */
+int rbim_resident_threads(int64_t L);
+
 /*
  * Initial spins of n_chains chains (reference initial_spins,
  * src/rbim/swendsen_wang.py:56-78): hot != 0 draws Philox stream 2 of each
@@ -151,7 +156,8 @@ int rbim_label_wrap(int64_t L, int n_lattices, const uint8_t *occ, int32_t *labe
  * rbim_resident_max_l()).  This is the engine behind many calls of the
  * reference's run_single_realization (src/rbim/simulation.py:196-242) and
  * sw_sweep (src/rbim/swendsen_wang.py:103-172).  records may be NULL.
- * threads: CTA size (0 = default).  workspace: rbim_batched_workspace_bytes()
+ * threads: CTA size, 64, 128, 256, 512 or 1024 (0 = rbim_resident_threads(l_max)).
+ * workspace: rbim_batched_workspace_bytes()
  * bytes (the work-queue counter).
  */
 size_t rbim_batched_workspace_bytes(void);

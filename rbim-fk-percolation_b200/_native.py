@@ -58,6 +58,7 @@ EXPORTED_SYMBOLS = (
     "rbim_abi_version",
     "rbim_plane_words",
     "rbim_resident_max_l",
+    "rbim_resident_threads",
     "rbim_init_spins",
     "rbim_activate_workspace_bytes",
     "rbim_activate",
@@ -93,6 +94,8 @@ def _declare(l):
     l.rbim_plane_words.argtypes = [c_i64]
     l.rbim_resident_max_l.restype = c_int
     l.rbim_resident_max_l.argtypes = []
+    l.rbim_resident_threads.restype = c_int
+    l.rbim_resident_threads.argtypes = [c_i64]
     l.rbim_init_spins.restype = c_int
     l.rbim_init_spins.argtypes = [p, c_int, p, c_int, p]
     l.rbim_activate_workspace_bytes.restype = c_size
@@ -168,15 +171,16 @@ def resident_max_l() -> int:
 def engine_buckets(Ls, r_max: int, c_max: int):
     """Launch bucket of every lattice size: ``(kind, key)`` with kind 0 resident, 1 cluster, 2 plain.
 
-    Resident lattices are bucketed by power-of-two size class (the resident
-    launch sizes its CTAs for the bucket's largest L), cluster lattices by
-    CTAs per cluster; buckets sort in launch order.
+    Resident lattices are bucketed by their default CTA size
+    (``rbim_resident_threads``; the launch sizes its CTAs and shared memory
+    for the bucket's largest L), cluster lattices by CTAs per cluster;
+    buckets sort in launch order.
     """
     out = []
     for L in Ls:
         L = int(L)
         if L <= r_max:
-            out.append((0, max(4, (L - 1).bit_length())))
+            out.append((0, int(lib().rbim_resident_threads(L))))
         elif L <= c_max:
             out.append((1, int(lib().rbim_cluster_size(L))))
         else:

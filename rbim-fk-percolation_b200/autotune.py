@@ -25,7 +25,7 @@ import numpy as np
 __all__ = ["CANDIDATES", "size_class", "enabled", "enable", "disable", "tuned_threads", "tune", "cache"]
 
 #: CTA sizes the resident engine accepts.
-CANDIDATES = (128, 256, 512, 1024)
+CANDIDATES = (64, 128, 256, 512, 1024)
 
 _lock = threading.Lock()
 _cache: Dict[str, int] = {}

@@ -118,6 +118,12 @@ int64_t rbim_plane_words(int64_t L) { return L < 1 ? 0 : plane_words(L); }
 
 int rbim_resident_max_l(void) { return rbim::resident_max_l(); }
 
+int rbim_resident_threads(int64_t L)
+{
+    if (L < 3 || L > rbim::resident_max_l()) return 0;
+    return rbim::resident_default_threads((int)L);
+}
+
 int rbim_init_spins(const rbim_chain_t *chains, int n_chains, uint32_t *spin_pool, int hot, void *stream)
 {
     if (n_chains < 0) return fail(RBIM_ERR_INVALID, "n_chains must be >= 0");
@@ -201,8 +207,8 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
     if (!aligned16(spin_pool) || !aligned16(coupling_pool))
         return fail(RBIM_ERR_INVALID, "spin and coupling pools must be 16-byte aligned");
     if (workspace_bytes < rbim_batched_workspace_bytes()) return fail(RBIM_ERR_INVALID, "workspace too small");
-    if (threads != 0 && threads != 128 && threads != 256 && threads != 512 && threads != 1024)
-        return fail(RBIM_ERR_INVALID, "threads must be 0, 128, 256, 512 or 1024 (got %d)", threads);
+    if (threads != 0 && threads != 64 && threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+        return fail(RBIM_ERR_INVALID, "threads must be 0, 64, 128, 256, 512 or 1024 (got %d)", threads);
     cudaError_t e = rbim::launch_resident_sweeps(chains, n_chains, (int)l_max, spin_pool, coupling_pool,
                                                  (long long *)acc_int, acc_f64, records, n_sweeps, threads, 0,
                                                  (int *)workspace, status, (cudaStream_t)stream);
