@@ -52,6 +52,12 @@ def test_host_only_queries(rb):
     assert lib.rbim_plain_workspace_bytes(1024) >= 8 * 1024 * 1024
     assert lib.rbim_activate_workspace_bytes(2) == 0
     assert lib.rbim_batched_workspace_bytes() >= 4
+    # Default CTA size of the resident engine: a supported size, never
+    # shrinking as L grows, 0 outside the engine's range.
+    sizes = [lib.rbim_resident_threads(L) for L in range(3, lmax + 1)]
+    assert set(sizes) <= {64, 128, 256, 512, 1024}
+    assert sizes == sorted(sizes)
+    assert lib.rbim_resident_threads(2) == 0 and lib.rbim_resident_threads(lmax + 1) == 0
 
 
 def test_argument_errors_are_reported_without_device_work(rb):
