@@ -233,44 +233,146 @@ __device__ __forceinline__ void phase_heads(const Lat<WT> &t, uint32_t warp, uin
     }
 }
 
-// (b) Unions across occupied x-bonds (including the x seam, image offset
-// (1,0)).  A bond is skipped when the bond one step lower in y is occupied and
-// both y-bonds joining them are occupied: it then closes an elementary
-// plaquette, which is contractible and already connected.
+// Occupied x-bonds of word w that need a union, the x seam included.  A bond
+// is skipped when the bond one step lower in y is occupied and both y-bonds
+// joining them are occupied: it then closes an elementary plaquette, which is
+// contractible and already connected (across the x seam the plaquette
+// crosses the seam once each way).
 template <class WT>
-__device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t warp, uint32_t nwarps, uint32_t tid,
-                                            uint32_t nthreads)
+__device__ __forceinline__ uint32_t x_union_need(const Lat<WT> &t, uint32_t w)
 {
-    const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
+    const uint32_t oh = t.OH[w];
+    if (!oh) return 0u;
     Plane OVp{t.OV};
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t oh = t.OH[w];
-        if (!oh) continue;
-        const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
-        const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
-        const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
-        const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
-        uint32_t s = (w << 5) + g.N + g.L - 1u;
-        s %= g.N;
-        const uint32_t prev_ovx = extract32(OVp, s, g);
-        const uint32_t need = oh & ~(prev_oh & prev_ov & prev_ovx);
-        if ((need >> lane) & 1u) {
-            const uint32_t n = (w << 5) + lane;
-            uint32_t b = n + g.L;
-            int ex = 0;
-            if (b >= g.N) {
-                b -= g.N;
+    const uint32_t ohp = w ? t.OH[w - 1u] : 0u;
+    const uint32_t ov = OVp(w), ovp = w ? OVp(w - 1u) : 0u;
+    const uint32_t prev_oh = (oh << 1) | (ohp >> 31);
+    const uint32_t prev_ov = (ov << 1) | (ovp >> 31);
+    uint32_t s = (w << 5) + g.N + g.L - 1u;
+    s %= g.N;
+    return oh & ~(prev_oh & prev_ov & extract32(OVp, s, g));
+}
+
+// One endpoint walk of a union: the current node, its word as last read, and
+// the summed image offset from the walk's start to the node.
+template <class WT>
+struct Walk {
+    typename WT::T w;
+    uint32_t node;
+    int ax, ay;
+};
+
+// One path-halving step (src/rbim/_unionfind.py:59-88: the offsets of the
+// skipped link are folded into the halved pointer).  Returns true, without
+// moving, when the walk stands on a node whose word says it is a root.
+template <class WT>
+__device__ __forceinline__ bool walk_step(const UF<WT> &uf, Walk<WT> &k)
+{
+    const uint32_t p = WT::parent(k.w);
+    if (p == k.node) return true;
+    const typename WT::T wp = uf.ld(p);
+    const uint32_t gp = WT::parent(wp);
+    if (gp != p) {
+        const int nx = WT::ox(k.w) + WT::ox(wp), ny = WT::oy(k.w) + WT::oy(wp);
+        uf.st(k.node, WT::make(gp, nx, ny));
+        k.ax += nx;
+        k.ay += ny;
+        k.node = gp;
+        k.w = uf.ld(gp);
+    } else {
+        k.ax += WT::ox(k.w);
+        k.ay += WT::oy(k.w);
+        k.node = p;
+        k.w = wp;
+    }
+    return false;
+}
+
+// (b) Unions across occupied x-bonds (including the x seam, image offset
+// (1,0)) and the y seam ((0,1)), with the loop-winding test of
+// src/rbim/_unionfind.py:104-124.  The x-bonds run as one flat loop per
+// thread: thread t owns the bit ranges t, t + T, ... (each word cut into a
+// power-of-two number of ranges, so that every thread of a large grid gets
+// work), both endpoint walks advance one step per iteration, and the thread
+// takes its next bond as soon as the current union is done, so that a
+// thread's cost is the sum of its own walks instead of a per-word maximum
+// over its warp.  The larger root is hooked under the smaller with a CAS on
+// its (self, 0, 0) word; a lost race resumes both walks from where they stand.
+template <class WT>
+__device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint32_t nthreads)
+{
+    using T = typename WT::T;
+    const Geom &g = t.g;
+    const UF<WT> &uf = t.uf;
+    uint32_t lg = 0;
+    while (lg < 5u && ((unsigned long long)g.NW << (lg + 1u)) <= nthreads) ++lg;
+    const uint32_t bits = 32u >> lg, items = g.NW << lg;
+    const uint32_t seg = bits == 32u ? 0xFFFFFFFFu : (1u << bits) - 1u;
+    uint32_t item = tid, pending = 0, base = 0;
+    Walk<WT> a{}, b{};
+    int ex = 0;
+    bool fetch = true;
+    const unsigned long long cap = 64ull * g.N + 4096ull;
+    for (unsigned long long it = 0;; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrUnionCap);
+            break;
+        }
+        if (fetch) {
+            while (!pending && item < items) {
+                const uint32_t w = item >> lg;
+                pending = x_union_need(t, w) & (seg << ((item & ((1u << lg) - 1u)) * bits));
+                base = w << 5;
+                item += nthreads;
+            }
+            if (!pending) break;
+            const uint32_t n = base + (uint32_t)(__ffs(pending) - 1);
+            pending &= pending - 1u;
+            uint32_t m = n + g.L;
+            ex = 0;
+            if (m >= g.N) {
+                m -= g.N;
                 ex = 1;
             }
-            uf_union<WT>(t.uf, n, b, ex, 0, t.wrap, t.cap, t.err);
+            a = Walk<WT>{uf.ld(n), n, 0, 0};
+            b = Walk<WT>{uf.ld(m), m, 0, 0};
+            fetch = false;
+        }
+        const bool ra = walk_step<WT>(uf, a);
+        const bool rb = walk_step<WT>(uf, b);
+        if (!(ra && rb)) continue;
+        if (a.node == b.node) {
+            int f = 0;
+            if (WT::nonzero(ex + b.ax - a.ax)) f |= 1;
+            if (WT::nonzero(b.ay - a.ay)) f |= 2;
+            if (f) atomicOr(t.wrap, f);
+            fetch = true;
+        } else if (a.node < b.node) {
+            const T expect = WT::make(b.node, 0, 0);
+            const T old = uf.cas(b.node, expect, WT::make(a.node, a.ax - ex - b.ax, a.ay - b.ay));
+            if (old == expect) {
+                fetch = true;
+            } else {
+                b.w = old;
+                a.w = uf.ld(a.node);
+            }
+        } else {
+            const T expect = WT::make(a.node, 0, 0);
+            const T old = uf.cas(a.node, expect, WT::make(b.node, b.ax + ex - a.ax, b.ay - a.ay));
+            if (old == expect) {
+                fetch = true;
+            } else {
+                a.w = old;
+                b.w = uf.ld(b.node);
+            }
         }
     }
     // y seam: (x, L-1) -> (x, 0) with image offset (0, 1).
     for (uint32_t x = tid; x < g.L; x += nthreads) {
         if ((t.SEAMV[x >> 5] >> (x & 31u)) & 1u) {
-            const uint32_t a = x * g.L + g.L - 1u;
-            uf_union<WT>(t.uf, a, x * g.L, 0, 1, t.wrap, t.cap, t.err);
+            const uint32_t a0 = x * g.L + g.L - 1u;
+            uf_union<WT>(t.uf, a0, x * g.L, 0, 1, t.wrap, t.cap, t.err);
         }
     }
 }
@@ -313,7 +415,12 @@ __device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uin
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
     // Two words per iteration (w0 and w1 = w0 + nwarps) keep two independent
-    // chains of loads in flight.
+    // chains of loads in flight.  With `count`, each warp carries the size of
+    // one cluster -- the one of its first site -- across its words and adds
+    // it once at the end: when one cluster spans most of the lattice its root
+    // would otherwise take an atomic per word from every warp, all on one
+    // address.
+    uint32_t carried = 0xFFFFFFFFu, carried_n = 0;
     for (uint32_t w0 = warp; w0 < g.NW; w0 += 2u * nwarps) {
         const uint32_t w1 = w0 + nwarps;
         const uint32_t n0 = (w0 << 5) + lane, n1 = (w1 << 5) + lane;
@@ -335,18 +442,24 @@ __device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uin
             if (lane == 1 && w1 < g.NW) t.S[w1] = ns1 & g.valid(w1);
         }
         if (count) {
-            const uint32_t live0 = __ballot_sync(0xFFFFFFFFu, ok0);
-            if (ok0) {
-                const uint32_t grp = __match_any_sync(live0, r0);
+            // Lane 0's site of the warp's first word exists (w0 < NW).
+            if (carried == 0xFFFFFFFFu) carried = __shfl_sync(0xFFFFFFFFu, r0, 0);
+            const uint32_t c0 = __ballot_sync(0xFFFFFFFFu, ok0 && r0 == carried);
+            const uint32_t c1 = __ballot_sync(0xFFFFFFFFu, ok1 && r1 == carried);
+            carried_n += __popc(c0) + __popc(c1);
+            const uint32_t rest0 = __ballot_sync(0xFFFFFFFFu, ok0) & ~c0;
+            if ((rest0 >> lane) & 1u) {
+                const uint32_t grp = __match_any_sync(rest0, r0);
                 if (lane == (uint32_t)(__ffs(grp) - 1)) t.uf.add(r0, WT::count_inc(__popc(grp)));
             }
-            const uint32_t live1 = __ballot_sync(0xFFFFFFFFu, ok1);
-            if (ok1) {
-                const uint32_t grp = __match_any_sync(live1, r1);
+            const uint32_t rest1 = __ballot_sync(0xFFFFFFFFu, ok1) & ~c1;
+            if ((rest1 >> lane) & 1u) {
+                const uint32_t grp = __match_any_sync(rest1, r1);
                 if (lane == (uint32_t)(__ffs(grp) - 1)) t.uf.add(r1, WT::count_inc(__popc(grp)));
             }
         }
     }
+    if (count && lane == 0 && carried_n) t.uf.add(carried, WT::count_inc(carried_n));
 }
 
 // (d) Unsatisfied bonds and down spins over words first, first+stride, ...

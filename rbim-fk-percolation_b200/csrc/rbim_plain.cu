@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_heads(PlainArgs a)
 __global__ void __launch_bounds__(kPlainThreads) k_plain_union(PlainArgs a)
 {
     if (!chain_phase(a.chain)) return;
-    phase_union<Word64>(plain_lat(a), gwarp(), gnwarps(), gtid(), gnthreads());
+    phase_union<Word64>(plain_lat(a), gtid(), gnthreads());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_roots(PlainArgs a)
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_label_heads(PlainWs ws,
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_union(PlainWs ws, uint32_t L)
 {
-    phase_union<Word64>(label_lat(ws, L), gwarp(), gnwarps(), gtid(), gnthreads());
+    phase_union<Word64>(label_lat(ws, L), gtid(), gnthreads());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_roots(PlainWs ws, uint32_t L)
