@@ -212,12 +212,19 @@ __device__ __forceinline__ void uf_atomic_add(unsigned short *p, unsigned short 
 }
 
 // Storage for one lattice's union-find words: a base pointer into shared or
-// global memory (generic addressing covers both).
+// global memory (generic addressing covers both).  `ldc` is a load that may be
+// served by the SM's L1 (global memory only) and so may return an older value
+// than the latest store of another SM.  The walks use it: pointers only ever
+// move to ancestors and a node that stopped being a root never becomes one
+// again, so a stale word still names an ancestor with the right image offset,
+// and every hook is a CAS that re-checks the root word in L2.  It takes the
+// hot words near a large cluster's root off a single L2 slice.
 template <class WT>
 struct UF {
     using T = typename WT::T;
     T *w;
     __device__ __forceinline__ T ld(uint32_t i) const { return *((volatile T *)(w + i)); }
+    __device__ __forceinline__ T ldc(uint32_t i) const { return __ldca(w + i); }
     __device__ __forceinline__ void st(uint32_t i, T v) const { *((volatile T *)(w + i)) = v; }
     __device__ __forceinline__ T cas(uint32_t i, T expect, T v) const { return atomicCAS(w + i, expect, v); }
     __device__ __forceinline__ void add(uint32_t i, T v) const { uf_atomic_add(w + i, v); }

@@ -46,6 +46,8 @@ struct UF<Word16> {
         asm volatile("ld.volatile.shared.u16 %0, [%1];" : "=h"(v) : "r"(sa + 2u * i) : "memory");
         return v;
     }
+    // Shared memory is coherent within the CTA: the same load as ld.
+    __device__ __forceinline__ T ldc(uint32_t i) const { return ld(i); }
     __device__ __forceinline__ void st(uint32_t i, T v) const
     {
         asm volatile("st.volatile.shared.u16 [%0], %1;" ::"r"(sa + 2u * i), "h"(v) : "memory");
@@ -71,30 +73,6 @@ __device__ __forceinline__ uint32_t last_row_mask(const Geom &g, uint32_t w)
     const uint32_t v = g.valid(w);
     if (n0 >= first) return v;
     return ~((1u << (first - n0)) - 1u) & v;
-}
-
-// Work slices.  Pointer chasing has data-dependent length, so the union and
-// root phases run as flat per-thread loops that take one pointer step per
-// iteration and fetch the next item as soon as the current one is done; a
-// thread's cost is then the sum of its items' steps rather than a per-round
-// maximum over the warp.  Thread t owns the bit ranges t, t + T, t + 2T, ...
-// where each word is cut into `seg` equal ranges (seg is a power of two
-// chosen so that small lattices still give every thread work).
-struct Slices {
-    uint32_t seg_log2, bits, items;
-    __device__ __forceinline__ uint32_t word(uint32_t i) const { return i >> seg_log2; }
-    __device__ __forceinline__ uint32_t mask(uint32_t i) const
-    {
-        const uint32_t s = i & ((1u << seg_log2) - 1u);
-        return (bits == 32u ? 0xFFFFFFFFu : ((1u << bits) - 1u)) << (s * bits);
-    }
-};
-
-__device__ __forceinline__ Slices make_slices(uint32_t NW, uint32_t nthreads)
-{
-    uint32_t lg = 0;
-    while (lg < 5u && (NW << (lg + 1u)) <= nthreads) ++lg;
-    return Slices{lg, 32u >> lg, NW << lg};
 }
 
 // Occupied x-bonds of word w that need a union: off the x seam, and not

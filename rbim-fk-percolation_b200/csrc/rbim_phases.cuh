@@ -233,6 +233,30 @@ __device__ __forceinline__ void phase_heads(const Lat<WT> &t, uint32_t warp, uin
     }
 }
 
+// Work slices.  Pointer chasing has data-dependent length, so the union and
+// root phases run as flat per-thread loops that take one pointer step per
+// iteration and fetch the next item as soon as the current one is done; a
+// thread's cost is then the sum of its items' steps rather than a per-round
+// maximum over the warp.  Thread t owns the bit ranges t, t + T, t + 2T, ...
+// where each word is cut into `seg` equal ranges (seg is a power of two
+// chosen so that small lattices still give every thread work).
+struct Slices {
+    uint32_t seg_log2, bits, items;
+    __device__ __forceinline__ uint32_t word(uint32_t i) const { return i >> seg_log2; }
+    __device__ __forceinline__ uint32_t mask(uint32_t i) const
+    {
+        const uint32_t s = i & ((1u << seg_log2) - 1u);
+        return (bits == 32u ? 0xFFFFFFFFu : ((1u << bits) - 1u)) << (s * bits);
+    }
+};
+
+__device__ __forceinline__ Slices make_slices(uint32_t NW, uint32_t nthreads)
+{
+    uint32_t lg = 0;
+    while (lg < 5u && (NW << (lg + 1u)) <= nthreads) ++lg;
+    return Slices{lg, 32u >> lg, NW << lg};
+}
+
 // Occupied x-bonds of word w that need a union, the x seam included.  A bond
 // is skipped when the bond one step lower in y is occupied and both y-bonds
 // joining them are occupied: it then closes an elementary plaquette, which is
@@ -265,13 +289,15 @@ struct Walk {
 
 // One path-halving step (src/rbim/_unionfind.py:59-88: the offsets of the
 // skipped link are folded into the halved pointer).  Returns true, without
-// moving, when the walk stands on a node whose word says it is a root.
+// moving, when the walk stands on a node whose word says it is a root.  The
+// words are read with UF::ldc; a word that is out of date only makes the walk
+// stop short on a former root, where the CAS of the union fails and reloads.
 template <class WT>
 __device__ __forceinline__ bool walk_step(const UF<WT> &uf, Walk<WT> &k)
 {
     const uint32_t p = WT::parent(k.w);
     if (p == k.node) return true;
-    const typename WT::T wp = uf.ld(p);
+    const typename WT::T wp = uf.ldc(p);
     const uint32_t gp = WT::parent(wp);
     if (gp != p) {
         const int nx = WT::ox(k.w) + WT::ox(wp), ny = WT::oy(k.w) + WT::oy(wp);
@@ -279,7 +305,7 @@ __device__ __forceinline__ bool walk_step(const UF<WT> &uf, Walk<WT> &k)
         k.ax += nx;
         k.ay += ny;
         k.node = gp;
-        k.w = uf.ld(gp);
+        k.w = uf.ldc(gp);
     } else {
         k.ax += WT::ox(k.w);
         k.ay += WT::oy(k.w);
@@ -292,12 +318,9 @@ __device__ __forceinline__ bool walk_step(const UF<WT> &uf, Walk<WT> &k)
 // (b) Unions across occupied x-bonds (including the x seam, image offset
 // (1,0)) and the y seam ((0,1)), with the loop-winding test of
 // src/rbim/_unionfind.py:104-124.  The x-bonds run as one flat loop per
-// thread: thread t owns the bit ranges t, t + T, ... (each word cut into a
-// power-of-two number of ranges, so that every thread of a large grid gets
-// work), both endpoint walks advance one step per iteration, and the thread
-// takes its next bond as soon as the current union is done, so that a
-// thread's cost is the sum of its own walks instead of a per-word maximum
-// over its warp.  The larger root is hooked under the smaller with a CAS on
+// thread over its work slices: both endpoint walks advance one step per
+// iteration, and the thread takes its next bond as soon as the current union
+// is done.  The larger root is hooked under the smaller with a CAS on
 // its (self, 0, 0) word; a lost race resumes both walks from where they stand.
 template <class WT>
 __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint32_t nthreads)
@@ -305,10 +328,7 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint
     using T = typename WT::T;
     const Geom &g = t.g;
     const UF<WT> &uf = t.uf;
-    uint32_t lg = 0;
-    while (lg < 5u && ((unsigned long long)g.NW << (lg + 1u)) <= nthreads) ++lg;
-    const uint32_t bits = 32u >> lg, items = g.NW << lg;
-    const uint32_t seg = bits == 32u ? 0xFFFFFFFFu : (1u << bits) - 1u;
+    const Slices sl = make_slices(g.NW, nthreads);
     uint32_t item = tid, pending = 0, base = 0;
     Walk<WT> a{}, b{};
     int ex = 0;
@@ -320,9 +340,9 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint
             break;
         }
         if (fetch) {
-            while (!pending && item < items) {
-                const uint32_t w = item >> lg;
-                pending = x_union_need(t, w) & (seg << ((item & ((1u << lg) - 1u)) * bits));
+            while (!pending && item < sl.items) {
+                const uint32_t w = sl.word(item);
+                pending = x_union_need(t, w) & sl.mask(item);
                 base = w << 5;
                 item += nthreads;
             }
@@ -335,8 +355,8 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint
                 m -= g.N;
                 ex = 1;
             }
-            a = Walk<WT>{uf.ld(n), n, 0, 0};
-            b = Walk<WT>{uf.ld(m), m, 0, 0};
+            a = Walk<WT>{uf.ldc(n), n, 0, 0};
+            b = Walk<WT>{uf.ldc(m), m, 0, 0};
             fetch = false;
         }
         const bool ra = walk_step<WT>(uf, a);
@@ -380,27 +400,69 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint
 // (c) Roots of the run heads.  Every parent pointer targets a head (heads
 // are the initial parents, roots are heads, and hooks and path halving only
 // move pointers to roots or grandparents), so once each head points straight
-// at its root, every site reaches its root in two steps.  The walk only
-// reads and each head's thread writes only its own word, so no final pointer
-// can be overwritten by a stale ancestor.  Roots are recorded in ROOT.
-// Returns this warp's number of roots.
+// at its root, every site reaches its root in two steps.  The walks only
+// read, and each head's word is written by the head's own thread alone, so
+// no final pointer can be overwritten by a stale ancestor.  A flat loop per
+// thread over the heads of its work slices, two walks in flight; roots are
+// recorded in ROOT, which must be zero on entry.  Returns this thread's
+// number of roots.
 template <class WT>
-__device__ __forceinline__ uint32_t phase_roots(const Lat<WT> &t, uint32_t warp, uint32_t nwarps)
+__device__ __forceinline__ bool next_head_of(const Lat<WT> &t, const Slices &sl, uint32_t nthreads, uint32_t &item,
+                                             uint32_t &pending, uint32_t &base, uint32_t &h)
 {
-    const uint32_t lane = threadIdx.x & 31u;
+    while (!pending && item < sl.items) {
+        const uint32_t w = sl.word(item);
+        pending = head_mask(t.OV, w, t.g.valid(w)) & sl.mask(item);
+        base = w << 5;
+        item += nthreads;
+    }
+    if (!pending) return false;
+    h = base + (uint32_t)(__ffs(pending) - 1);
+    pending &= pending - 1u;
+    return true;
+}
+
+template <class WT>
+__device__ __forceinline__ uint32_t phase_roots(const Lat<WT> &t, uint32_t tid, uint32_t nthreads)
+{
     const Geom &g = t.g;
-    uint32_t nroots = 0;
-    for (uint32_t w = warp; w < g.NW; w += nwarps) {
-        const uint32_t n = (w << 5) + lane;
-        const bool head = (head_mask(t.OV, w, g.valid(w)) >> lane) & 1u;
-        uint32_t r = n;
-        if (head) {
-            r = uf_root_ro<WT>(t.uf, n, t.cap, t.err);
-            if (r != n) t.uf.st(n, WT::make(r, 0, 0));
+    const Slices sl = make_slices(g.NW, nthreads);
+    uint32_t item = tid, pending = 0, base = 0, nroots = 0;
+    uint32_t h0 = 0, h1 = 0;
+    bool a0 = next_head_of(t, sl, nthreads, item, pending, base, h0);
+    bool a1 = a0 && next_head_of(t, sl, nthreads, item, pending, base, h1);
+    uint32_t x0 = h0, x1 = h1;
+    const unsigned long long cap = 64ull * g.N + 4096ull;
+    for (unsigned long long it = 0; a0 || a1; ++it) {
+        if (it >= cap) {
+            atomicOr(t.err, kErrFindCap);
+            break;
         }
-        const uint32_t roots = __ballot_sync(0xFFFFFFFFu, head && r == n);
-        if (lane == 0) t.ROOT[w] = roots;
-        nroots += __popc(roots);
+        const uint32_t p0 = a0 ? WT::parent(t.uf.ldc(x0)) : x0;
+        const uint32_t p1 = a1 ? WT::parent(t.uf.ldc(x1)) : x1;
+        const bool r0 = a0 && p0 == x0, r1 = a1 && p1 == x1;
+        x0 = p0;
+        x1 = p1;
+        if (r0) {
+            if (x0 != h0) {
+                t.uf.st(h0, WT::make(x0, 0, 0));
+            } else {
+                atomicOr(t.ROOT + (h0 >> 5), 1u << (h0 & 31u));
+                ++nroots;
+            }
+            a0 = next_head_of(t, sl, nthreads, item, pending, base, h0);
+            x0 = h0;
+        }
+        if (r1) {
+            if (x1 != h1) {
+                t.uf.st(h1, WT::make(x1, 0, 0));
+            } else {
+                atomicOr(t.ROOT + (h1 >> 5), 1u << (h1 & 31u));
+                ++nroots;
+            }
+            a1 = next_head_of(t, sl, nthreads, item, pending, base, h1);
+            x1 = h1;
+        }
     }
     return nroots;
 }
@@ -408,7 +470,9 @@ __device__ __forceinline__ uint32_t phase_roots(const Lat<WT> &t, uint32_t warp,
 // (c') Every site: root = parent of parent (after phase_roots), pointed at
 // directly; the spin is flipped with its cluster's flip bit; with `count` the
 // root words accumulate the cluster size in their offset field
-// (warp-aggregated with match_any).
+// (warp-aggregated with match_any).  A site's parent is a head and a head's
+// parent is its root, so the parent fields read here are final and the loads
+// may come from L1 (the count adds change only the root words' upper half).
 template <class WT>
 __device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uint32_t nwarps, bool flip, bool count)
 {
@@ -426,10 +490,10 @@ __device__ __forceinline__ void phase_sites(const Lat<WT> &t, uint32_t warp, uin
         const uint32_t n0 = (w0 << 5) + lane, n1 = (w1 << 5) + lane;
         const bool ok0 = n0 < g.N, ok1 = n1 < g.N;
         uint32_t r0 = 0, r1 = 0, p0 = 0, p1 = 0;
-        if (ok0) p0 = WT::parent(t.uf.ld(n0));
-        if (ok1) p1 = WT::parent(t.uf.ld(n1));
-        if (ok0) r0 = WT::parent(t.uf.ld(p0));
-        if (ok1) r1 = WT::parent(t.uf.ld(p1));
+        if (ok0) p0 = WT::parent(t.uf.ldc(n0));
+        if (ok1) p1 = WT::parent(t.uf.ldc(n1));
+        if (ok0) r0 = WT::parent(t.uf.ldc(p0));
+        if (ok1) r1 = WT::parent(t.uf.ldc(p1));
         if (ok0 && r0 != p0) t.uf.st(n0, WT::make(r0, 0, 0));
         if (ok1 && r1 != p1) t.uf.st(n1, WT::make(r1, 0, 0));
         if (flip) {

@@ -157,10 +157,13 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_activate(PlainArgs a)
     phase_activate<Word64>(t, rng, gwarp(), gnwarps(), gtid(), gnthreads());
 }
 
+// Run heads; also clears the ROOT plane for the root walks that follow.
 __global__ void __launch_bounds__(kPlainThreads) k_plain_heads(PlainArgs a)
 {
     if (!chain_phase(a.chain)) return;
-    phase_heads<Word64>(plain_lat(a), gwarp(), gnwarps());
+    const Lat<Word64> t = plain_lat(a);
+    for (uint32_t w = gtid(); w < t.g.NW; w += gnthreads()) t.ROOT[w] = 0u;
+    phase_heads<Word64>(t, gwarp(), gnwarps());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_union(PlainArgs a)
@@ -173,7 +176,9 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_roots(PlainArgs a)
 {
     if (!chain_phase(a.chain)) return;
     const Lat<Word64> t = plain_lat(a);
-    const uint32_t nr = phase_roots<Word64>(t, gwarp(), gnwarps());
+    uint32_t nr = phase_roots<Word64>(t, gtid(), gnthreads());
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nr += __shfl_xor_sync(0xFFFFFFFFu, nr, o);
     if ((threadIdx.x & 31u) == 0 && nr) atomicAdd(&a.ws.sc->nroots, nr);
 }
 
@@ -200,7 +205,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
             roots &= roots - 1u;
             const uint32_t r = (w << 5) + b;
             const unsigned long long key =
-                ((unsigned long long)Word64::count(t.uf.ld(r)) << 32) | (0xFFFFFFFFull - r);
+                ((unsigned long long)Word64::count(t.uf.ldc(r)) << 32) | (0xFFFFFFFFull - r);
             top2_merge(k1, k2, key, 0ull);
         }
     }
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_measure3(PlainArgs a)
     int mc = 0;
     for (uint32_t w = gwarp(); w < t.g.NW; w += gnwarps()) {
         const uint32_t n = (w << 5) + lane;
-        const bool in = n < t.g.N && Word64::parent(t.uf.ld(n)) == g1;
+        const bool in = n < t.g.N && Word64::parent(t.uf.ldc(n)) == g1;
         const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
         if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
     }
@@ -364,7 +369,9 @@ __device__ __forceinline__ Lat<Word64> label_lat(const PlainWs &ws, uint32_t L)
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_heads(PlainWs ws, uint32_t L)
 {
-    phase_heads<Word64>(label_lat(ws, L), gwarp(), gnwarps());
+    const Lat<Word64> t = label_lat(ws, L);
+    for (uint32_t w = gtid(); w < t.g.NW; w += gnthreads()) t.ROOT[w] = 0u;
+    phase_heads<Word64>(t, gwarp(), gnwarps());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_union(PlainWs ws, uint32_t L)
@@ -374,7 +381,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_label_union(PlainWs ws,
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_roots(PlainWs ws, uint32_t L)
 {
-    phase_roots<Word64>(label_lat(ws, L), gwarp(), gnwarps());
+    (void)phase_roots<Word64>(label_lat(ws, L), gtid(), gnthreads());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_label_finalize(PlainWs ws, uint32_t L)
