@@ -243,8 +243,10 @@ def run_single_realization(L: int, J: np.ndarray, temperature: float, *, n_sweep
     """One realization at one temperature on the GPU (reference ``simulation.py:148-242``).
 
     ``engine``: ``"plain"`` (global-memory engine, one lattice per launch
-    sequence), ``"batched"`` (resident engine) or ``"auto"`` (resident when L
-    fits on chip).
+    sequence), ``"batched"`` (resident or cluster engine, one CTA or one
+    cluster for the lattice) or ``"auto"`` (plain for L > 128, where the whole
+    grid on one lattice beats one CTA or one cluster; batched otherwise).
+    Every engine gives the same result.
     """
     spb = _check_run(n_sweeps, n_bins)
     hot = _check_start(start)

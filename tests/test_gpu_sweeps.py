@@ -175,3 +175,18 @@ def test_sw_sweep_api_matches_oracle(rb, orc):
                 res.second_size, res.wraps_x, res.wraps_y) == (r[0], r[1], r[2], r[3], r[4], r[5], bool(r[7]),
                                                                bool(r[8]))
         assert np.array_equal(spins, ref.astype(np.int64))
+
+
+@pytest.mark.parametrize("L", [100, 160])
+def test_single_realization_engines_agree(rb, L):
+    """run_single_realization gives the same sums on every engine; engine="auto" takes the plain engine for one
+    lattice with L > PLAIN_SINGLE_MIN_L and the resident engine below."""
+    J = _couplings(L, 0.08, L)
+    out = {e: rb.run_single_realization(L, J, 2.1, n_sweeps=24, n_therm=4, n_bins=4, seed=11, engine=e)
+           for e in ("auto", "plain", "batched")}
+    for e in ("plain", "batched"):
+        for k, v in out["auto"].primitives.items():
+            assert np.array_equal(np.float64(v).view(np.uint64), np.float64(out[e].primitives[k]).view(np.uint64)), (e, k)
+        for k, v in out["auto"].bin_primitives.items():
+            assert np.array_equal(np.asarray(v, np.float64).view(np.uint64),
+                                  np.asarray(out[e].bin_primitives[k], np.float64).view(np.uint64)), (e, k)
