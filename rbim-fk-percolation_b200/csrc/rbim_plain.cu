@@ -27,6 +27,8 @@ struct PlainScratch {
     unsigned long long g1;
     unsigned long long s1;
     unsigned long long s2;
+    unsigned int done1;  // CTAs of k_plain_measure1 finished this sweep
+    unsigned int done3;  // CTAs of k_plain_measure3 finished this sweep
 };
 
 struct PlainWs {
@@ -233,24 +235,30 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
             a.ws.top2[2 * blockIdx.x + 1] = b2;
         }
     }
-}
-
-__global__ void __launch_bounds__(1024) k_plain_measure2(PlainArgs a, int nblocks)
-{
-    if (chain_phase(a.chain) != 2) return;
-    unsigned long long k1 = 0, k2 = 0;
-    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) top2_merge(k1, k2, a.ws.top2[2 * i], a.ws.top2[2 * i + 1]);
+    // The last CTA to finish merges every CTA's top two, in place of a
+    // separate single-CTA launch: each CTA publishes its pair, fences and
+    // takes a ticket; the CTA with the last ticket reads all pairs from L2.
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&a.ws.sc->done1, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    k1 = 0;
+    k2 = 0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+        top2_merge(k1, k2, __ldcg(a.ws.top2 + 2 * i), __ldcg(a.ws.top2 + 2 * i + 1));
     warp_top2(k1, k2);
-    __shared__ unsigned long long s1[32], s2[32];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (lane == 0) {
         s1[warp] = k1;
         s2[warp] = k2;
     }
     __syncthreads();
     if (warp == 0) {
-        const uint32_t nw = blockDim.x >> 5;
-        unsigned long long b1 = lane < nw ? s1[lane] : 0ull, b2 = lane < nw ? s2[lane] : 0ull;
+        unsigned long long b1 = lane < kPlainThreads / 32 ? s1[lane] : 0ull;
+        unsigned long long b2 = lane < kPlainThreads / 32 ? s2[lane] : 0ull;
         warp_top2(b1, b2);
         if (lane == 0) {
             PlainScratch *sc = a.ws.sc;
@@ -261,29 +269,14 @@ __global__ void __launch_bounds__(1024) k_plain_measure2(PlainArgs a, int nblock
     }
 }
 
-__global__ void __launch_bounds__(kPlainThreads) k_plain_measure3(PlainArgs a)
+// End of a sweep (one thread): the sweep's record and bin sums from the
+// scratch, the status word, the sweep counter, and a zeroed scratch for the
+// next sweep.  The scratch is read through L2 (volatile): other CTAs of the
+// calling kernel added to it.
+__device__ void plain_end(const PlainArgs &a, int ph)
 {
-    if (chain_phase(a.chain) != 2) return;
-    if (a.ws.sc->nroots <= 1) return;
-    const Lat<Word64> t = plain_lat(a);
-    const uint32_t g1 = (uint32_t)a.ws.sc->g1;
-    const uint32_t lane = threadIdx.x & 31u;
-    int mc = 0;
-    for (uint32_t w = gwarp(); w < t.g.NW; w += gnwarps()) {
-        const uint32_t n = (w << 5) + lane;
-        const bool in = n < t.g.N && Word64::parent(t.uf.ldc(n)) == g1;
-        const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
-        if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
-    }
-    if (lane == 0 && mc) atomicAdd((unsigned long long *)&a.ws.sc->mc, (unsigned long long)(long long)mc);
-}
-
-__global__ void k_plain_end(PlainArgs a)
-{
-    const int ph = chain_phase(a.chain);
-    if (!ph) return;
     rbim_chain_t *c = a.chain;
-    PlainScratch *sc = a.ws.sc;
+    const volatile PlainScratch *sc = a.ws.sc;
     if (ph == 2) {
         const long long N = c->L * c->L;
         const long long M = N - 2ll * (long long)sc->downs;
@@ -296,7 +289,8 @@ __global__ void k_plain_end(PlainArgs a)
         }
         if (mc < 0) mc = -mc;
         const long long E = 2ll * (long long)sc->unsat - 2ll * N;
-        const int wx = sc->wrap & 1, wy = (sc->wrap >> 1) & 1;
+        const int wrap = sc->wrap;
+        const int wx = wrap & 1, wy = (wrap >> 1) & 1;
         const long long idx = (long long)(c->sweep - (uint64_t)c->n_therm);
         const long long bin = idx / c->sweeps_per_bin;
         Acc acc;
@@ -315,10 +309,43 @@ __global__ void k_plain_end(PlainArgs a)
             row[7] = wy;
         }
     }
-    if (sc->err) atomicOr(a.status, sc->err);
+    const int err = sc->err;
+    if (err) atomicOr(a.status, err);
     c->sweep = c->sweep + 1;
     PlainScratch z{};
-    *sc = z;
+    *a.ws.sc = z;
+}
+
+// Magnetisation of the largest cluster (measured sweeps with more than one
+// cluster), then, in the last CTA to finish, the end of the sweep: every CTA
+// adds its share, fences and takes a ticket, so the last ticket sees all
+// shares.  Thermalisation sweeps run only the ticket and the end.
+__global__ void __launch_bounds__(kPlainThreads) k_plain_measure3(PlainArgs a)
+{
+    const int ph = chain_phase(a.chain);
+    if (!ph) return;
+    if (ph == 2 && a.ws.sc->nroots > 1) {
+        const Lat<Word64> t = plain_lat(a);
+        const uint32_t g1 = (uint32_t)a.ws.sc->g1;
+        const uint32_t lane = threadIdx.x & 31u;
+        int mc = 0;
+        for (uint32_t w = gwarp(); w < t.g.NW; w += gnwarps()) {
+            const uint32_t n = (w << 5) + lane;
+            const bool in = n < t.g.N && Word64::parent(t.uf.ldc(n)) == g1;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
+            if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
+        }
+        if (lane == 0 && mc) atomicAdd((unsigned long long *)&a.ws.sc->mc, (unsigned long long)(long long)mc);
+    }
+    // Every thread fences its own adds before the CTA's ticket is taken.
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (atomicAdd(&a.ws.sc->done3, 1u) == gridDim.x - 1u) {
+            __threadfence();
+            plain_end(a, ph);
+        }
+    }
 }
 
 // Labelling of a frozen occupation mask (bond-order bytes) through the plain
@@ -458,9 +485,7 @@ cudaError_t launch_plain_sweeps(rbim_chain_t *chain, uint32_t *spin_pool, const 
         k_plain_roots<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_finalize<<<grid, kPlainThreads, 0, stream>>>(a);
         k_plain_measure1<<<grid, kPlainThreads, 0, stream>>>(a);
-        k_plain_measure2<<<1, 1024, 0, stream>>>(a, grid);
         k_plain_measure3<<<grid, kPlainThreads, 0, stream>>>(a);
-        k_plain_end<<<1, 1, 0, stream>>>(a);
     }
     return cudaGetLastError();
 }
