@@ -15,7 +15,7 @@ itself as ``rbim_b200`` in ``sys.modules``.
 
 import sys as _sys
 
-from . import _native, autotune
+from . import _native, autotune, seeding
 from ._native import RbimError
 from .clusters import (
     activate_bonds,
@@ -32,6 +32,7 @@ from .disorder import (
     frustrated_plaquettes,
     frustration_density,
     generate_disorder,
+    generate_disorders,
     load_disorder,
     save_disorder,
 )
@@ -67,6 +68,7 @@ __all__ = [
     "site_index",
     "couplings_from_disorder",
     "generate_disorder",
+    "generate_disorders",
     "load_disorder",
     "save_disorder",
     "frustrated_plaquettes",

@@ -19,10 +19,11 @@ from typing import Dict, Iterable, Optional, Sequence
 
 import numpy as np
 
-from .disorder import generate_disorder
+from .disorder import generate_disorders
 from .engine import ChainSet, ChainSpec, chain_key
 from .lattice import couplings_from_disorder
 from .packing import pack_couplings
+from .seeding import child_keys
 
 __all__ = [
     "OBSERVABLES",
@@ -316,7 +317,7 @@ def plan_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_
     disorder_seeds, run_seeds = seed_sequence.spawn(2)
     if disorder is None:
         disorder_rng = np.random.default_rng(disorder_seeds)
-        realizations = [generate_disorder(L, p, disorder_rng) for _ in range(n_realizations)]
+        realizations = generate_disorders(L, p, disorder_rng, n_realizations)
     else:
         realizations = list(disorder)[:n_realizations]
         if len(realizations) < n_realizations:
@@ -327,8 +328,7 @@ def plan_temperature_scan(L: int, p: float, temperatures: Sequence[float], *, n_
     for J in couplings:
         if J.size != 2 * L * L:
             raise ValueError(f"disorder realization has {J.size // 2} sites, expected {L * L}")
-    children = run_seeds.spawn(len(temperatures) * len(couplings))
-    keys = np.array([chain_key(c) for c in children], dtype=np.uint64)
+    keys = child_keys(run_seeds, len(temperatures) * len(couplings))
     return ScanPlan(L=L, p=p, temperatures=temperatures, couplings=couplings, keys=keys, n_sweeps=n_sweeps,
                     n_therm=n_therm, n_bins=n_bins, sweeps_per_bin=spb, seed=seed, hot=hot, start=start,
                     measure_percolation=measure_percolation)

@@ -71,6 +71,39 @@ def test_disorder_generation_draws_like_the_reference(rb):
         rb.generate_disorder(4, 1.5, rng)
 
 
+@pytest.mark.parametrize("L,p,n", [(3, 0.05, 4), (17, 0.5, 3), (64, 1e-9, 2), (256, 0.1, 20), (9, 0.0, 2),
+                                   (9, 1.0, 2)])
+def test_batched_disorder_equals_the_reference_calls(rb, L, p, n):
+    """generate_disorders (integer compares on the raw PCG64 draws, drawn in parallel chunks when many) gives the
+    couplings of n reference calls ``rng.random((L, L)) < p`` (J_h, then J_v) in a row, and leaves the generator
+    where those calls leave it."""
+    a, b = np.random.default_rng(1000 + L), np.random.default_rng(1000 + L)
+    got = rb.disorder.generate_disorders(L, p, a, n)
+    for J_h, J_v in got:
+        u1, u2 = b.random((L, L)), b.random((L, L))
+        assert J_h.dtype == np.int8 and J_h.shape == (L, L)
+        assert np.array_equal(J_h, np.where(u1 < p, -1, 1)) and np.array_equal(J_v, np.where(u2 < p, -1, 1))
+    assert a.bit_generator.state == b.bit_generator.state
+
+
+def test_child_keys_equal_spawned_children(rb):
+    """Vectorised SeedSequence children: the same keys as spawn() + chain_key for many parents."""
+    seeding = rb.seeding
+    for seed in (0, 1, 12345, 2**32 + 7, 2**70 + 3, 2**127 + 11, [1, 2, 3], [2**40, 5]):
+        for depth in (0, 1):
+            a = np.random.SeedSequence(seed)
+            b = np.random.SeedSequence(seed)
+            if depth:
+                a, b = a.spawn(5)[3], b.spawn(5)[3]
+            a, b = a.spawn(2)[1], b.spawn(2)[1]
+            want = np.array([rb.chain_key(c) for c in a.spawn(257)], dtype=np.uint64)
+            assert np.array_equal(seeding.child_keys(b, 257), want), (seed, depth)
+            b.spawn(257)
+            more = np.array([rb.chain_key(c) for c in a.spawn(5)], dtype=np.uint64)
+            assert np.array_equal(seeding.child_keys(b, 5), more), (seed, depth)
+    assert seeding.child_keys(np.random.SeedSequence(3), 0).size == 0
+
+
 def test_disorder_file_round_trip(rb, tmp_path):
     J_h, J_v = rb.generate_disorder(7, 0.2, np.random.default_rng(1))
     path = tmp_path / rb.default_disorder_filename(7, 0.2, 3)
