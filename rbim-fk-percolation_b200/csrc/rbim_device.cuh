@@ -299,34 +299,6 @@ __device__ __forceinline__ uint32_t uf_root_ro(const UF<WT> &uf, uint32_t n, uin
     return node;
 }
 
-// Root only (no offsets), with path halving.
-template <class WT>
-__device__ __forceinline__ uint32_t uf_root(const UF<WT> &uf, uint32_t n, uint32_t cap, int *err)
-{
-    using T = typename WT::T;
-    uint32_t node = n;
-    T w = uf.ld(node);
-    for (uint32_t it = 0;; ++it) {
-        const uint32_t p = WT::parent(w);
-        if (p == node) break;
-        if (it >= cap) {
-            atomicOr(err, kErrFindCap);
-            break;
-        }
-        const T wp = uf.ld(p);
-        const uint32_t gp = WT::parent(wp);
-        if (gp != p) {
-            uf.st(node, WT::make(gp, WT::ox(w) + WT::ox(wp), WT::oy(w) + WT::oy(wp)));
-            node = gp;
-            w = uf.ld(node);
-        } else {
-            node = p;
-            w = wp;
-        }
-    }
-    return node;
-}
-
 // Union across the bond a -> b whose seam crossing is (ex, ey).  Sets bit 0
 // (x) / bit 1 (y) of *wrap when the bond closes a loop that winds.  The larger
 // root is hooked under the smaller with a CAS on its (self, 0, 0) word.
