@@ -164,6 +164,23 @@ def profiled_traffic(path):
     return None
 
 
+def profiled_sm_throughput(path):
+    """sm__throughput (percent of peak) of the workload's kernel from the committed ncu summary, or None.
+
+    The on-chip engines keep every sweep's state in shared memory, so their
+    limit is SM issue and shared-memory latency rather than HBM; this is the
+    figure that shows how close the kernel runs to that limit.
+    """
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("sm__throughput (pct of peak)"):
+                    return float(line.split(")", 1)[1].split("%")[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def cpu_baseline(L, temps, ps, seconds=10.0, threads=0):
     """The oracle's restatement of the reference sweep on the host cores: lattice-sweeps/s."""
     import oracle
@@ -461,6 +478,7 @@ def main():
     achieved = BYTES_PER_SITE_UPDATE * site_updates_launch / launch_s / 1e9
     kernel = "k_resident_sweeps" if L <= rb._native.resident_max_l() else "k_cluster_sweeps"
     traffic = profiled_traffic(os.path.join(PROFILES, f"{kernel}_L{L}.txt"))
+    sm_pct = profiled_sm_throughput(os.path.join(PROFILES, f"{kernel}_L{L}.txt"))
 
     # Plain engine: one lattice per launch sequence, same L.
     plain = None
@@ -558,7 +576,9 @@ def main():
         "site_updates_per_s": value * L * L,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "bytes_per_site_update": BYTES_PER_SITE_UPDATE, "kernel": kernel},
+                     "bytes_per_site_update": BYTES_PER_SITE_UPDATE, "kernel": kernel,
+                     "sm_throughput_pct_of_peak": sm_pct,
+                     "sm_throughput_source": f"ncu summary profiles/{kernel}_L{L}.txt" if sm_pct is not None else None},
         "clocks": clocks.summary(),
         "gpu_launches": args.steps,
         "e2e": e2e,
