@@ -28,6 +28,7 @@ __all__ = [
 
 
 _PARALLEL_DRAWS = 1 << 20  # below this many draws one thread is as fast
+_GROUP_DRAWS = 1 << 25     # most raw draws held at once by generate_disorders
 
 
 def _raw_draws(rng: np.random.Generator, n: int) -> np.ndarray:
@@ -122,9 +123,17 @@ def generate_disorders(L: int, p: float, rng: Optional[np.random.Generator] = No
         rng = np.random.default_rng()
     n = int(n)
     if n > 0 and _fast_path(rng, p):
-        neg = _pcg64_compare(rng, n * 2 * L * L, p).view(np.int8).reshape(n, 2, L, L)
-        J = np.int8(1) - (neg + neg)
-        return [(J[k, 0], J[k, 1]) for k in range(n)]
+        # Groups of realizations of at most _GROUP_DRAWS draws (256 MB of raw
+        # draws), one after the other, so the stream order is kept.
+        per = 2 * L * L
+        group = max(1, _GROUP_DRAWS // per)
+        out = []
+        for k0 in range(0, n, group):
+            m = min(group, n - k0)
+            neg = _pcg64_compare(rng, m * per, p).view(np.int8).reshape(m, 2, L, L)
+            J = np.int8(1) - (neg + neg)
+            out += [(J[k, 0], J[k, 1]) for k in range(m)]
+        return out
     out = []
     for _ in range(n):
         J_h = np.where(rng.random((L, L)) < p, -1, 1).astype(np.int8)

@@ -86,6 +86,17 @@ def test_batched_disorder_equals_the_reference_calls(rb, L, p, n):
     assert a.bit_generator.state == b.bit_generator.state
 
 
+def test_batched_disorder_in_groups(rb, monkeypatch):
+    """Large batches are drawn in groups of realizations, one after the other: same couplings, same end state."""
+    monkeypatch.setattr(rb.disorder, "_GROUP_DRAWS", 3000)
+    a, b = np.random.default_rng(7), np.random.default_rng(7)
+    got = rb.disorder.generate_disorders(20, 0.2, a, 9)
+    for J_h, J_v in got:
+        u1, u2 = b.random((20, 20)), b.random((20, 20))
+        assert np.array_equal(J_h, np.where(u1 < 0.2, -1, 1)) and np.array_equal(J_v, np.where(u2 < 0.2, -1, 1))
+    assert a.bit_generator.state == b.bit_generator.state
+
+
 def test_child_keys_equal_spawned_children(rb):
     """Vectorised SeedSequence children: the same keys as spawn() + chain_key for many parents."""
     seeding = rb.seeding
