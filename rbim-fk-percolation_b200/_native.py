@@ -176,16 +176,15 @@ def engine_buckets(Ls, r_max: int, c_max: int):
     for the bucket's largest L), cluster lattices by CTAs per cluster;
     buckets sort in launch order.
     """
-    out = []
-    for L in Ls:
-        L = int(L)
+    key_of = {}
+    for L in set(int(L) for L in Ls):
         if L <= r_max:
-            out.append((0, int(lib().rbim_resident_threads(L))))
+            key_of[L] = (0, int(lib().rbim_resident_threads(L)))
         elif L <= c_max:
-            out.append((1, int(lib().rbim_cluster_size(L))))
+            key_of[L] = (1, int(lib().rbim_cluster_size(L)))
         else:
-            out.append((2, 0))
-    return out
+            key_of[L] = (2, 0)
+    return [key_of[int(L)] for L in Ls]
 
 
 def cluster_max_l() -> int:

@@ -159,15 +159,19 @@ class ChainSet:
         self.slot = np.empty(self.n, dtype=np.int64)
         self.slot[order] = np.arange(self.n)
         self.buckets = []  # (kind, first slot, count, l_max)
-        for k in sorted(set(keys)):
-            members = [i for i in range(self.n) if keys[i] == k]
-            first = int(min(self.slot[i] for i in members))
-            self.buckets.append((k[0], first, len(members), int(max(Ls[i] for i in members))))
+        groups = {}
+        for i, k in enumerate(keys):
+            groups.setdefault(k, []).append(i)
+        for k in sorted(groups):
+            members = np.array(groups[k], dtype=np.int64)
+            self.buckets.append((k[0], int(self.slot[members].min()), len(members), int(Ls[members].max())))
         self.plain_only = [int(i) for i in order if keys[i][0] == 2]
 
         desc = np.zeros(self.n, dtype=_native.CHAIN_DTYPE)
         desc["key"] = [s.key for s in self.specs]
-        desc["thr"] = [threshold(s.beta) for s in self.specs]
+        thr_of = {}
+        desc["thr"] = [thr_of[s.beta] if s.beta in thr_of else thr_of.setdefault(s.beta, threshold(s.beta))
+                       for s in self.specs]
         desc["spin_off"] = s_off
         desc["coupling_off"] = c_off[[s.realization for s in self.specs]]
         desc["acc_off"] = a_off
