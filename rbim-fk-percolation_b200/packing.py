@@ -59,7 +59,10 @@ def pack_couplings(J: np.ndarray, L: int) -> np.ndarray:
         raise ValueError(f"expected {2 * L * L} couplings, got {j.size}")
     if not np.all((j == 1) | (j == -1)):
         raise ValueError("couplings must be +-1")
-    return np.concatenate([pack_plane(j[0::2] == -1, L), pack_plane(j[1::2] == -1, L)])
+    # Each (J_h, J_v) pair of int8 read as one little-endian uint16: the sign
+    # bit of J_h is bit 7, that of J_v bit 15 (contiguous, no strided pass).
+    u = np.ascontiguousarray(j, dtype=np.int8).view("<u2")
+    return np.concatenate([pack_plane((u & 0x0080) != 0, L), pack_plane((u & 0x8000) != 0, L)])
 
 
 def unpack_couplings(words: np.ndarray, L: int) -> np.ndarray:
