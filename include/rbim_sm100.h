@@ -181,6 +181,11 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
 int rbim_cluster_max_l(void);
 /* CTAs per cluster the cluster engine uses for an L x L lattice (0 if none). */
 int rbim_cluster_size(int64_t L);
+/* Threads per CTA of that plan (512 with half-size tiles or 1024; 0 if none).
+ * A call of rbim_sweeps_clustered runs every lattice in the plan of its l_max,
+ * so callers that mix sizes group lattices by (rbim_cluster_size,
+ * rbim_cluster_threads). */
+int rbim_cluster_threads(int64_t L);
 int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
                           const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
                           int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream);

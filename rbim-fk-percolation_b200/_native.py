@@ -70,6 +70,7 @@ EXPORTED_SYMBOLS = (
     "rbim_sweeps_plain",
     "rbim_cluster_max_l",
     "rbim_cluster_size",
+    "rbim_cluster_threads",
     "rbim_sweeps_clustered",
     "rbim_noalloc_max_l",
     "rbim_sweeps_plain_noalloc",
@@ -118,6 +119,8 @@ def _declare(l):
     l.rbim_cluster_max_l.argtypes = []
     l.rbim_cluster_size.restype = c_int
     l.rbim_cluster_size.argtypes = [c_i64]
+    l.rbim_cluster_threads.restype = c_int
+    l.rbim_cluster_threads.argtypes = [c_i64]
     l.rbim_sweeps_clustered.restype = c_int
     l.rbim_sweeps_clustered.argtypes = [p, c_int, c_i64, p, p, p, p, p, c_int, p, p, c_size, p]
     l.rbim_noalloc_max_l.restype = c_int
@@ -169,19 +172,20 @@ def resident_max_l() -> int:
 
 
 def engine_buckets(Ls, r_max: int, c_max: int):
-    """Launch bucket of every lattice size: ``(kind, key)`` with kind 0 resident, 1 cluster, 2 plain.
+    """Launch bucket of every lattice size: a tuple ``(kind, ...)`` with kind 0 resident, 1 cluster, 2 plain.
 
     Resident lattices are bucketed by their default CTA size
     (``rbim_resident_threads``; the launch sizes its CTAs and shared memory
-    for the bucket's largest L), cluster lattices by CTAs per cluster;
-    buckets sort in launch order.
+    for the bucket's largest L), cluster lattices by CTAs per cluster and CTA
+    size (``rbim_cluster_size``, ``rbim_cluster_threads``: a launch runs every
+    lattice in the plan of its largest L); buckets sort in launch order.
     """
     key_of = {}
     for L in set(int(L) for L in Ls):
         if L <= r_max:
             key_of[L] = (0, int(lib().rbim_resident_threads(L)))
         elif L <= c_max:
-            key_of[L] = (1, int(lib().rbim_cluster_size(L)))
+            key_of[L] = (1, int(lib().rbim_cluster_size(L)), int(lib().rbim_cluster_threads(L)))
         else:
             key_of[L] = (2, 0)
     return [key_of[int(L)] for L in Ls]

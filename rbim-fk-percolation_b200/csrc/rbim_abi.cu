@@ -252,6 +252,13 @@ int rbim_cluster_size(int64_t L)
     return (int)rbim::cluster_size_for((uint32_t)L);
 }
 
+int rbim_cluster_threads(int64_t L)
+{
+    if (L <= rbim::resident_max_l() || L > 65535) return 0;
+    const rbim::ClusterPlan plan = rbim::cluster_plan((uint32_t)L);
+    return plan.C ? (int)plan.threads : 0;
+}
+
 int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uint32_t *spin_pool,
                           const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64, int32_t *records,
                           int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream)

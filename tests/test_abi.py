@@ -58,6 +58,13 @@ def test_host_only_queries(rb):
     assert set(sizes) <= {64, 128, 256, 512, 1024}
     assert sizes == sorted(sizes)
     assert lib.rbim_resident_threads(2) == 0 and lib.rbim_resident_threads(lmax + 1) == 0
+    # Cluster plans: CTA size 512 (half-size tiles) or 1024 wherever a cluster size exists.
+    for L in range(lmax + 1, 1025):
+        c, t = lib.rbim_cluster_size(L), lib.rbim_cluster_threads(L)
+        assert (c == 0) == (t == 0) and t in (0, 512, 1024), L
+    assert lib.rbim_cluster_threads(lmax) == 0
+    assert {lib.rbim_cluster_threads(L) for L in (300, 420)} == {512, 1024}
+    assert lib.rbim_cluster_size(300) == lib.rbim_cluster_size(420)
 
 
 def test_argument_errors_are_reported_without_device_work(rb):
