@@ -97,3 +97,16 @@ def test_packing_matches_the_documented_layout(rb):
     spins[[0, 5, 31, 32, 35]] = -1
     w = rb.packing.pack_spins(spins, L)
     assert w[0] == (1 << 0) | (1 << 5) | (1 << 31) and w[1] == (1 << 0) | (1 << 3)
+
+
+def test_engine_buckets_split_modes(rb):
+    """Launch buckets: resident lattices by default CTA size, cluster lattices by (CTAs per cluster, CTA size),
+    the rest plain; keys sort in launch order."""
+    nat = rb._native
+    r_max = nat.lib().rbim_resident_max_l()
+    Ls = [16, 32, 48, 200, 300, 420, 2000]
+    keys = nat.engine_buckets(Ls, r_max, 1024)
+    assert keys[0] == keys[1] == (0, 64) and keys[2] == (0, 128) and keys[3][0] == 0
+    assert keys[4][:2] == keys[5][:2] and keys[4] != keys[5]  # same cluster size, different CTA size
+    assert keys[6] == (2, 0)
+    assert sorted(keys) == [keys[i] for i in sorted(range(len(Ls)), key=lambda i: keys[i])]
