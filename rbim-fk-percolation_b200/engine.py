@@ -21,11 +21,18 @@ import numpy as np
 from . import _native
 from .packing import threshold, unpack_spins, words_for
 
-__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_MIN_L"]
+__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_MIN_L", "auto_engine"]
 
 #: A set of one lattice runs on the plain engine under ``engine="auto"`` when
 #: its L exceeds this (measured on B200: below it one resident CTA is faster).
 PLAIN_SINGLE_MIN_L = 128
+
+
+def auto_engine(specs) -> str:
+    """The engine ``engine="auto"`` picks for a set of chains: ``"plain"`` for one lattice with
+    L > PLAIN_SINGLE_MIN_L (the whole grid on one lattice beats one CTA or one cluster), else ``"batched"``."""
+    specs = list(specs)
+    return "plain" if len(specs) == 1 and specs[0].L > PLAIN_SINGLE_MIN_L else "batched"
 
 
 def _torch():
@@ -325,7 +332,7 @@ class ChainSet:
         other set on the batched engines.  Results are the same either way.
         """
         if engine == "auto":
-            engine = "plain" if len(self.specs) == 1 and self.specs[0].L > PLAIN_SINGLE_MIN_L else "batched"
+            engine = auto_engine(self.specs)
         if engine not in ("batched", "plain"):
             raise ValueError(f"engine must be 'auto', 'batched' or 'plain', got {engine!r}")
         while self.remaining() > 0:

@@ -155,6 +155,16 @@ def test_threshold(rb):
     assert rb.bond_activation_probability(100.0) == pytest.approx(1.0)
 
 
+def test_auto_engine_choice(rb):
+    """engine="auto": the plain engine for a single lattice of L > PLAIN_SINGLE_MIN_L, batched otherwise."""
+    eng = rb.engine
+    spec = lambda L: rb.ChainSpec(L=L, realization=0, key=1, beta=0.5, n_therm=0, n_bins=1, sweeps_per_bin=1)
+    m = eng.PLAIN_SINGLE_MIN_L
+    assert eng.auto_engine([spec(m + 1)]) == "plain" and eng.auto_engine([spec(1024)]) == "plain"
+    assert eng.auto_engine([spec(m)]) == "batched" and eng.auto_engine([spec(16)]) == "batched"
+    assert eng.auto_engine([spec(1024), spec(1024)]) == "batched"
+
+
 def test_chain_keys_follow_seed_sequences(rb):
     ss = np.random.SeedSequence(0)
     _, run = ss.spawn(2)
