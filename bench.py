@@ -14,12 +14,16 @@ timed region).
 Also reported: ``e2e`` (the same metric through the public
 ``run_temperature_scan``, host disorder generation, copies and the jackknife
 included), the plain one-lattice-per-launch engine on the same lattice size,
-the roofline of the resident kernel against the measured HBM bandwidth,
-clocks sampled during the timed region, and the CPU baseline (the oracle's
-C restatement of the reference sweep on the host cores).
+the other configurations (the reference's L = 32 scan, L = 64 batched vs
+plain, the L = 512 slice, the whole uneven-size mix with concurrent bucket
+launches, one L = 1024 lattice for 2,000 sweeps), a serving load curve with
+the same requests run alone for comparison, the roofline of the resident
+kernel against the measured HBM bandwidth, clocks sampled during the timed
+region, and the CPU baseline (the oracle's C restatement of the reference
+sweep on the host cores, on chains of the same workload).
 
 ``--impl reference`` times only that CPU implementation (rank 0), on the same
-metric, with all host threads.
+metric, config and chains, with all host threads.
 """
 
 from __future__ import annotations
@@ -40,51 +44,57 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_SITE_UPDATE = 8.5  # packed spins r+w, packed couplings r, one int32 cluster id w+r
 PROFILES = os.path.join(ROOT, "profiles")
+METRIC = "L=256 SW sweeps/s batched vs plain on 1 B200 (obs within 2σ); scan p99 latency"
+C4_SIZES = (32, 48, 64, 96, 128, 192, 256, 512)
+C4_PS = (0.02, 0.05, 0.08, 0.10)
+
+
+def c4_realizations(L: int) -> int:
+    """Realizations per (L, p) of the uneven-size configuration: 4096 (32/L)^2 rounded up to 8."""
+    return int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
 
 
 def workload(name: str):
     if name == "c4_L256":
-        L = 256
-        ps = [0.02, 0.05, 0.08, 0.10]
-        n_real = int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
-        temps = np.linspace(1.2, 2.4, 32)
-    elif name == "c3_L64":
-        L = 64
-        ps = [0.05]
-        n_real = 256
-        temps = np.linspace(1.0, 3.0, 64)
-    elif name == "c4_L512":
-        L = 512
-        ps = [0.02, 0.05, 0.08, 0.10]
-        n_real = int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
-        temps = np.linspace(1.2, 2.4, 32)
-    elif name == "c2_L1024":
-        L = 1024
-        ps = [0.10]
-        n_real = 4
-        temps = np.linspace(1.5, 1.7, 32)
-    else:
-        raise SystemExit(f"unknown workload {name}")
-    return L, ps, n_real, temps
+        return 256, list(C4_PS), c4_realizations(256), np.linspace(1.2, 2.4, 32)
+    if name == "c3_L64":
+        return 64, [0.05], 256, np.linspace(1.0, 3.0, 64)
+    if name == "c4_L512":
+        return 512, list(C4_PS), c4_realizations(512), np.linspace(1.2, 2.4, 32)
+    if name == "c2_L1024":
+        return 1024, [0.10], 4, np.linspace(1.5, 1.7, 32)
+    raise SystemExit(f"unknown workload {name}")
 
 
-def build_chains(rb, L, ps, n_real, temps, seed, n_total):
-    """Chains (T-major per p, as the reference orders tasks) and packed couplings."""
-    specs, couplings = [], []
+def workload_config(args, L, ps, n_real, temps):
+    """The ``config`` of the JSON line: the workload only, identical for the engine and the reference arm."""
+    return {"workload": args.workload, "L": L, "p": list(ps), "realizations_per_p": n_real,
+            "temperatures": [float(temps[0]), float(temps[-1]), len(temps)], "chains": len(ps) * n_real * len(temps),
+            "sweeps_per_step": args.sweeps_per_step, "measured": True, "seed": args.seed,
+            "l2": "flushed between steps (256 MB write)", "parallelism": f"independent chains x{args.gpus}"}
+
+
+def build_chains(rb, L, ps, n_real, temps, seed, n_total, keep_bonds=False):
+    """Chains (T-major per p, as the reference orders tasks), packed couplings and, on request, the bond couplings.
+
+    Per p: ``SeedSequence([seed, p index]).spawn(2)`` gives the disorder and the run seeds; realizations are drawn
+    with the reference's generator calls, and chain k's key is that of run-seed child k.
+    """
+    specs, couplings, bonds = [], [], []
     for pi, p in enumerate(ps):
-        ss = np.random.SeedSequence([seed, pi])
-        dseed, rseed = ss.spawn(2)
-        drng = np.random.default_rng(dseed)
+        dseed, rseed = np.random.SeedSequence([seed, pi]).spawn(2)
         base = len(couplings)
-        for _ in range(n_real):
-            J_h, J_v = rb.generate_disorder(L, p, drng)
-            couplings.append(rb.packing.pack_couplings(rb.couplings_from_disorder(J_h, J_v), L))
-        kids = rseed.spawn(len(temps) * n_real)
-        for k, child in enumerate(kids):
+        for J_h, J_v in rb.generate_disorders(L, p, np.random.default_rng(dseed), n_real):
+            J = rb.couplings_from_disorder(J_h, J_v)
+            couplings.append(rb.packing.pack_couplings(J, L))
+            if keep_bonds:
+                bonds.append(J)
+        keys = rb.seeding.child_keys(rseed, len(temps) * n_real)
+        for k in range(len(temps) * n_real):
             t_index, r = divmod(k, n_real)
-            specs.append(rb.ChainSpec(L=L, realization=base + r, key=rb.chain_key(child), beta=1.0 / temps[t_index],
+            specs.append(rb.ChainSpec(L=L, realization=base + r, key=int(keys[k]), beta=1.0 / temps[t_index],
                                       n_therm=0, n_bins=1, sweeps_per_bin=n_total))
-    return specs, couplings
+    return (specs, couplings, bonds) if keep_bonds else (specs, couplings)
 
 
 class ClockSampler:
@@ -152,59 +162,92 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(path):
-    """DRAM bytes per launch of the workload's kernel from the committed ncu summary, or None."""
+def profiled_figure(path, prefix):
+    """A figure from a committed ncu summary: the first number after ``prefix`` on its line, or None."""
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch_scaled:"):
-                    return float(line.split(":", 1)[1])
-    except OSError:
+                if line.strip().startswith(prefix):
+                    rest = line.strip()[len(prefix):].lstrip(" :=")
+                    return float(rest.split()[0].rstrip("%"))
+    except (OSError, ValueError, IndexError):
         pass
     return None
 
 
-def profiled_sm_throughput(path):
-    """sm__throughput (percent of peak) of the workload's kernel from the committed ncu summary, or None.
-
-    The on-chip engines keep every sweep's state in shared memory, so their
-    limit is SM issue and shared-memory latency rather than HBM; this is the
-    figure that shows how close the kernel runs to that limit.
-    """
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.strip().startswith("sm__throughput (pct of peak)"):
-                    return float(line.split(")", 1)[1].split("%")[0])
-    except (OSError, ValueError):
-        pass
-    return None
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle's restatement of the reference sweep, on chains of the workload itself.
+# ---------------------------------------------------------------------------
+def cpu_sample(rb, L, ps, n_real, temps, seed, n_chains):
+    """``n_chains`` chains of the workload, evenly spread over its (p, temperature, realization) list."""
+    specs, _, bonds = build_chains(rb, L, ps, n_real, temps, seed, 1, keep_bonds=True)
+    pick = np.linspace(0, len(specs) - 1, n_chains).round().astype(int)
+    J = np.stack([bonds[specs[i].realization] for i in pick])
+    keys = np.array([specs[i].key for i in pick], dtype=np.uint64)
+    thrs = np.array([rb.packing.threshold(specs[i].beta) for i in pick], dtype=np.uint64)
+    return J, keys, thrs, [int(i) for i in pick]
 
 
-def cpu_baseline(L, temps, ps, seconds=10.0, threads=0):
-    """The oracle's restatement of the reference sweep on the host cores: lattice-sweeps/s."""
+def cpu_run(L, sample, sweeps, threads, spins=None):
+    """One timed run of ``sweeps`` measured sweeps of every sample chain, one chain per host thread."""
     import oracle
 
-    n_threads = threads or os.cpu_count() or 1
-    rng = np.random.default_rng(0)
-    J = np.stack([np.where(rng.random(2 * L * L) < ps[i % len(ps)], -1, 1).astype(np.int8) for i in range(n_threads)])
-    keys = np.arange(1, n_threads + 1, dtype=np.uint64)
-    thrs = np.array([int(np.floor(-np.expm1(-2.0 / temps[(7 * i) % len(temps)]) * 2**32)) for i in range(n_threads)],
-                    dtype=np.uint64)
-    # Calibrate: one sweep per chain, then size the sample to ~seconds.
+    J, keys, thrs, _ = sample
     t0 = time.perf_counter()
-    _, _, spins, used = oracle.run_chains(L, J, keys, thrs, n_therm=0, n_bins=1, sweeps_per_bin=1, n_threads=n_threads)
-    per = time.perf_counter() - t0
+    _, _, spins, used = oracle.run_chains(L, J, keys, thrs, n_therm=0, n_bins=1, sweeps_per_bin=sweeps,
+                                          spins=spins, n_threads=threads)
+    return time.perf_counter() - t0, spins, used
+
+
+def cpu_baseline(rb, L, ps, n_real, temps, seed, seconds=10.0, threads=0):
+    """Lattice-sweeps/s of the oracle on the host cores (a bounded sample of the workload's chains)."""
+    threads = threads or os.cpu_count() or 1
+    sample = cpu_sample(rb, L, ps, n_real, temps, seed, threads)
+    per, spins, used = cpu_run(L, sample, 1, threads)
     sweeps = max(1, int(seconds / max(per, 1e-4)))
-    t0 = time.perf_counter()
-    oracle.run_chains(L, J, keys, thrs, n_therm=0, n_bins=1, sweeps_per_bin=sweeps, spins=spins, n_threads=n_threads)
-    dt = time.perf_counter() - t0
-    value = n_threads * sweeps / dt
+    dt, _, used = cpu_run(L, sample, sweeps, threads, spins)
+    value = len(sample[1]) * sweeps / dt
     return {"value": value, "unit": "lattice-sweeps/s", "cores": used, "kind": "port",
-            "sample": f"{n_threads} chains of L={L} x {sweeps} measured sweeps, one chain per thread ({dt:.1f} s)"}
+            "sample": f"{len(sample[1])} chains of the workload (indices {sample[3][0]}..{sample[3][-1]}, evenly "
+                      f"spread over p and T), L={L}, {sweeps} measured sweeps each, one chain per thread "
+                      f"({dt:.1f} s)"}
 
 
-def time_sweeps(cs, n, plain=False):
+def run_reference(args, L, ps, n_real, temps):
+    """The reference arm: the oracle's C sweep on the host cores, on chains of the same workload and config."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    rb = importlib.import_module("rbim-fk-percolation_b200")
+    threads = os.cpu_count() or 1
+    sample = cpu_sample(rb, L, ps, n_real, temps, args.seed, threads)
+    per, spins, used = cpu_run(L, sample, 1, threads)
+    sweeps = max(1, int(args.ref_seconds / max(per, 1e-4)))
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt, spins, used = cpu_run(L, sample, sweeps, threads, spins)
+        if i >= args.warmup:
+            times.append(dt)
+    t = float(np.sum(times))
+    value = len(sample[1]) * sweeps * args.steps / t
+    line = {
+        "metric": METRIC, "value": value, "unit": "lattice-sweeps/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded +-J disorder from the reference's generator)",
+        "config": workload_config(args, L, ps, n_real, temps),
+        "site_updates_per_s": value * L * L,
+        "cpu_baseline": {"value": value, "unit": "lattice-sweeps/s", "cores": used, "kind": "port",
+                         "sample": f"each step: {len(sample[1])} chains of the workload (evenly spread over p and T), "
+                                   f"{sweeps} measured sweeps each, one chain per host thread"},
+        "e2e": {"value": value, "unit": "lattice-sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU legs.
+# ---------------------------------------------------------------------------
+def time_sweeps(cs, n, plain=False, concurrent=True):
     """Device time of n sweeps of every chain of a ChainSet (CUDA events on the current stream)."""
     import torch
 
@@ -214,22 +257,45 @@ def time_sweeps(cs, n, plain=False):
     if plain:
         cs.run_plain(n)
     else:
-        cs.run_batched(n)
+        cs.run_batched(n, concurrent=concurrent)
     e1.record()
     e1.synchronize()
     cs.check_status()
     return e0.elapsed_time(e1) / 1000.0
 
 
-def config_lines(rb, dev, seed):
-    """Throughput of the other configurations: batched vs plain at L = 64 (256 realizations x 64 T),
-    the L = 512 slice of the uneven-size mix and L = 1024 (cluster engine), one L = 1024 lattice."""
+def c2_line(rb, dev, seed, sweeps):
+    """One L = 1024 lattice (p = 0.10, T = 1.6) for ``sweeps`` measured sweeps, and the pure model at T_c, on the
+    engine ``engine="auto"`` picks for one lattice (the plain engine), device-timed; with E/N and <|m|>."""
     out = {}
+    L = 1024
+    tc = 2.0 / np.log(1.0 + np.sqrt(2.0))
+    for name, p, T in (("p0.10_T1.6", 0.10, 1.6), ("p0_Tc", 0.0, tc)):
+        specs, couplings = build_chains(rb, L, [p], 1, [T], seed, sweeps)
+        assert rb.engine.auto_engine(specs) == "plain"
+        cs = rb.ChainSet(specs, couplings, device=dev)
+        cs.init_spins(hot=True)
+        t = time_sweeps(cs, sweeps, plain=True)
+        ib, _ = cs.bins(0)
+        n = L * L
+        out[name] = {"p": p, "T": float(T), "sweeps": sweeps, "device_s": t, "lattice_sweeps_per_s": sweeps / t,
+                     "site_updates_per_s": sweeps * n / t, "us_per_sweep": 1e6 * t / sweeps,
+                     "E_per_site": float(ib[0, 0]) / sweeps / n, "abs_m": float(ib[0, 3]) / sweeps / n,
+                     "S1_over_N": float(ib[0, 5]) / sweeps / n}
+    out["engine"] = "plain (engine='auto' for one lattice with L > 128)"
+    out["note"] = "2,000 measured sweeps from a hot start, no thermalisation excluded"
+    return out
 
-    # The reference's own headline scan (plain method, small): L = 32, p = 0.05, 32 realizations x 40 T,
-    # 20,000 measured + 2,000 thermalisation sweeps, 20 bins, end to end through run_temperature_scan.
+
+def config_lines(rb, dev, seed, c2_sweeps):
+    """Throughput of the other configurations: the reference's L = 32 scan, batched vs plain at L = 64 (256
+    realizations x 64 T), the L = 512 slice of the uneven-size mix and L = 1024 (cluster engine, and one lattice
+    for 2,000 sweeps on the plain engine)."""
     import torch
 
+    out = {}
+    # The reference's own headline scan (plain method, small): L = 32, p = 0.05, 32 realizations x 40 T,
+    # 20,000 measured + 2,000 thermalisation sweeps, 20 bins, end to end through run_temperature_scan.
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     rb.run_temperature_scan(32, 0.05, np.linspace(1.0, 3.0, 40), n_realizations=32, n_sweeps=20000, n_therm=2000,
@@ -241,72 +307,63 @@ def config_lines(rb, dev, seed):
                           "site_updates_per_s": sweeps * 1024 / wall, "chains": 1280, "sweeps_per_chain": 22000,
                           "api": "run_temperature_scan, host disorder, copies and jackknife included"}
 
-    def chainset(L, p, n_real, temps, n_total, s):
-        specs, couplings = build_chains(rb, L, [p], n_real, temps, s, n_total)
+    def chainset(L, ps, n_real, temps, n_total, s):
+        specs, couplings = build_chains(rb, L, ps, n_real, temps, s, n_total)
         cs = rb.ChainSet(specs, couplings, device=dev)
         cs.init_spins(hot=True)
         return cs, specs, couplings
 
+    def plain_rate(specs, couplings, n):
+        pcs = rb.ChainSet(specs[:1], couplings[:1], device=dev)
+        pcs.init_spins(hot=True)
+        pcs.run_plain(3)
+        return n / time_sweeps(pcs, n, plain=True)
+
     # Batched, uniform size: L = 64, p = 0.05, 256 x 64 chains.
-    cs, specs, couplings = chainset(64, 0.05, 256, np.linspace(1.0, 3.0, 64), 1000, seed)
+    cs, specs, couplings = chainset(64, [0.05], 256, np.linspace(1.0, 3.0, 64), 1000, seed)
     cs.run_batched(3)
-    t = time_sweeps(cs, 10)
-    b = len(specs) * 10 / t
-    pcs = rb.ChainSet(specs[:1], couplings[:1], device=dev)
-    pcs.init_spins(hot=True)
-    pcs.run_plain(5)
-    pt = time_sweeps(pcs, 200, plain=True)
-    pv = 200 / pt
+    b = len(specs) * 10 / time_sweeps(cs, 10)
+    pv = plain_rate(specs, couplings, 200)
     out["c3_L64"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 4096,
                      "plain_lattice_sweeps_per_s": pv, "plain_site_updates_per_s": pv * 4096,
                      "batched_over_plain": b / pv, "chains": len(specs), "engine": "resident"}
-    del cs, pcs
+    del cs
     # The L = 512 slice of the uneven-size mix: 16 realizations x 4 p x 32 T.
-    specs, couplings = build_chains(rb, 512, [0.02, 0.05, 0.08, 0.10], 16, np.linspace(1.2, 2.4, 32), seed, 1000)
-    cs = rb.ChainSet(specs, couplings, device=dev)
-    cs.init_spins(hot=True)
+    cs, specs, couplings = chainset(512, list(C4_PS), 16, np.linspace(1.2, 2.4, 32), 1000, seed)
     cs.run_batched(1)
-    t = time_sweeps(cs, 3)
-    b = len(specs) * 3 / t
-    pcs = rb.ChainSet(specs[:1], couplings[:1], device=dev)
-    pcs.init_spins(hot=True)
-    pcs.run_plain(3)
-    pv = 50 / time_sweeps(pcs, 50, plain=True)
+    b = len(specs) * 3 / time_sweeps(cs, 3)
+    pv = plain_rate(specs, couplings, 50)
     out["c4_L512"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 512 * 512,
                       "plain_lattice_sweeps_per_s": pv, "batched_over_plain": b / pv, "chains": len(specs),
                       "engine": "cluster (4 CTAs per lattice)"}
-    del cs, pcs
-    # L = 1024: one lattice (p = 0.10, T = 1.6) on the plain and the cluster engine, and 128 lattices batched.
-    cs, specs, couplings = chainset(1024, 0.10, 4, np.linspace(1.5, 1.7, 32), 1000, seed)
+    del cs
+    # L = 1024: 128 lattices batched (cluster engine) and one lattice on the cluster engine.
+    cs, specs, couplings = chainset(1024, [0.10], 4, np.linspace(1.5, 1.7, 32), 1000, seed)
     cs.run_batched(1)
-    t = time_sweeps(cs, 3)
-    b = len(specs) * 3 / t
-    one = rb.ChainSet([rb.ChainSpec(L=1024, realization=0, key=specs[0].key, beta=1 / 1.6, n_therm=0, n_bins=1,
-                                    sweeps_per_bin=1000)], couplings[:1], device=dev)
+    b = len(specs) * 3 / time_sweeps(cs, 3)
+    one = rb.ChainSet(specs[:1], couplings[:1], device=dev)
     one.init_spins(hot=True)
     one.run_batched(2)
     ov = 20 / time_sweeps(one, 20)
-    one.run_plain(2)
-    pv = 20 / time_sweeps(one, 20, plain=True)
-    out["c2_L1024"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 1024 * 1024,
-                       "one_lattice_cluster_sweeps_per_s": ov, "one_lattice_plain_sweeps_per_s": pv,
-                       "batched_over_plain": b / pv, "chains": len(specs), "engine": "cluster (16 CTAs per lattice)"}
+    out["L1024_batched"] = {"batched_lattice_sweeps_per_s": b, "batched_site_updates_per_s": b * 1024 * 1024,
+                            "one_lattice_cluster_sweeps_per_s": ov, "chains": len(specs),
+                            "engine": "cluster (16 CTAs per lattice)"}
+    del cs, one
+    # The single-lattice configuration itself: one L = 1024 lattice, 2,000 sweeps.
+    out["c2_L1024"] = c2_line(rb, dev, seed, c2_sweeps)
     return out
 
 
 def c4_full_line(rb, dev, seed, sweeps=2):
     """The whole uneven-size configuration in one ChainSet: L in {32, 48, 64, 96, 128, 192, 256, 512},
     p in {0.02, 0.05, 0.08, 0.10}, 4096 (32/L)^2 realizations (rounded up to 8) x 32 temperatures per (L, p);
-    one run_batched call advances every lattice (one launch per size bucket)."""
-    import torch
-
+    each run_batched call advances every lattice, its bucket launches running concurrently (and, for
+    comparison, one after another)."""
     temps = np.linspace(1.2, 2.4, 32)
-    ps = [0.02, 0.05, 0.08, 0.10]
     t0 = time.perf_counter()
     specs, couplings = [], []
-    for L in (32, 48, 64, 96, 128, 192, 256, 512):
-        n_real = int(np.ceil(4096 * (32 / L) ** 2 / 8) * 8)
-        sp, cp = build_chains(rb, L, ps, n_real, temps, seed + L, 1000)
+    for L in C4_SIZES:
+        sp, cp = build_chains(rb, L, list(C4_PS), c4_realizations(L), temps, seed + L, 1000)
         base = len(couplings)
         for s_ in sp:
             s_.realization += base
@@ -317,17 +374,22 @@ def c4_full_line(rb, dev, seed, sweeps=2):
     setup = time.perf_counter() - t0
     sites = float(sum(s_.L * s_.L for s_ in specs))
     cs.run_batched(1)
-    t = time_sweeps(cs, sweeps)
-    return {"lattices": len(specs), "sites": sites, "sweeps": sweeps, "ms_per_sweep_of_all": 1e3 * t / sweeps,
-            "lattice_sweeps_per_s": len(specs) * sweeps / t, "site_updates_per_s": sites * sweeps / t,
-            "host_setup_s": setup, "launches_per_sweep": len(cs.buckets)}
+    t_conc = min(time_sweeps(cs, sweeps) for _ in range(2))
+    t_ser = time_sweeps(cs, sweeps, concurrent=False)
+    return {"lattices": len(specs), "sites": sites, "sweeps_per_call": sweeps,
+            "ms_per_sweep_of_all": 1e3 * t_conc / sweeps, "lattice_sweeps_per_s": len(specs) * sweeps / t_conc,
+            "site_updates_per_s": sites * sweeps / t_conc,
+            "serial_launches_ms_per_sweep_of_all": 1e3 * t_ser / sweeps,
+            "concurrent_over_serial": t_ser / t_conc, "host_setup_s": setup,
+            "launches_per_call": sum(1 for b in cs.buckets if b[0] != 2),
+            "launch_mode": "one launch per bucket, all buckets concurrent on forked streams (own queue counters)"}
 
 
-def serving_leg(rb, dev, seconds, rate, scale, seed, quantum):
-    """Poisson stream of temperature-scan requests (the serving configuration's distribution of L, p,
-    temperatures and realizations, sweeps scaled by `scale`) through the continuous-batching server."""
+def serving_requests(rb, seconds, rate, scale, seed):
+    """A seeded Poisson stream of scan requests with the serving configuration's distributions of L, p,
+    temperatures, realizations and sweeps (sweeps scaled by ``scale``, at least 10)."""
     rng = np.random.default_rng(seed)
-    arrivals, reqs, work = [], [], 0
+    arrivals, reqs, work = [], [], []
     t = 0.0
     while True:
         t += rng.exponential(1.0 / rate)
@@ -341,7 +403,13 @@ def serving_leg(rb, dev, seconds, rate, scale, seed, quantum):
                              n_realizations=n_r, n_sweeps=sweeps, n_bins=10, seed=int(rng.integers(2**31)))
         arrivals.append(t)
         reqs.append(req)
-        work += n_t * n_r * (sweeps + max(1, sweeps // 10)) * L * L
+        work.append(n_t * n_r * (sweeps + max(1, sweeps // 10)) * L * L)
+    return arrivals, reqs, work
+
+
+def serving_point(rb, dev, seconds, rate, scale, seed, quantum):
+    """Latency and throughput of one arrival rate through the continuous-batching server."""
+    arrivals, reqs, work = serving_requests(rb, seconds, rate, scale, seed)
     server = rb.ScanServer(device=dev, memory_bytes=8 << 30, quantum=quantum)
     with server:
         t0 = time.perf_counter()
@@ -356,33 +424,46 @@ def serving_leg(rb, dev, seconds, rate, scale, seed, quantum):
         t_end = time.perf_counter() - t0
     pct = server.latency_percentiles((50, 99))
     served = sum(c["site_updates"] for c in server.completed)
-    return {"p50_s": pct["p50"], "p99_s": pct["p99"], "requests": len(reqs), "arrival_window_s": seconds,
-            "rate_per_s": rate, "sweep_scale": scale, "quantum_sweeps": quantum, "wall_s": t_end,
-            "offered_site_updates_per_s": work / seconds, "served_site_updates_per_s": served / t_end,
-            "launches": server.launches}
+    return {"rate_per_s": rate, "requests": len(reqs), "p50_s": pct["p50"], "p99_s": pct["p99"],
+            "offered_site_updates_per_s": sum(work) / seconds, "served_site_updates_per_s": served / t_end,
+            "wall_s": t_end, "launches": server.launches}
 
 
-def run_reference(args, L, ps, temps, metric):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    values = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(L, temps, ps, seconds=args.ref_seconds)
-        if i >= args.warmup:
-            values.append(r["value"])
-    value = float(np.mean(values))
-    line = {
-        "metric": metric, "value": value, "unit": "lattice-sweeps/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * args.ref_seconds, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": args.workload, "L": L, "sample": "bounded CPU sample per step"},
-        "site_updates_per_s": value * L * L,
-        "cpu_baseline": dict(r, value=value),
-        "e2e": {"value": value, "unit": "lattice-sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+def serving_leg(rb, dev, args):
+    """Serving: a latency-vs-offered-load curve (the spec's request shapes, sweeps scaled by ``--serve-scale``,
+    arrival rates up to the spec's 20/s), and the stream's first requests each run alone, one after another,
+    through ``run_temperature_scan`` on the plain engine and on the batched engines."""
+    import torch
+
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    curve = [serving_point(rb, dev, args.serve_seconds, r, args.serve_scale, args.seed, args.serve_quantum)
+             for r in rates]
+    _, reqs, work = serving_requests(rb, args.serve_seconds, max(rates), args.serve_scale, args.seed)
+    alone = {}
+    sample = list(zip(reqs, work))[: args.serve_alone]
+    for engine in ("plain", "batched"):
+        t = 0.0
+        for req, _ in sample:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rb.run_temperature_scan(req.L, req.p, req.temperatures, n_realizations=req.n_realizations,
+                                    n_sweeps=req.n_sweeps, n_bins=req.n_bins, seed=req.seed, device=dev,
+                                    engine=engine)
+            torch.cuda.synchronize()
+            t += time.perf_counter() - t0
+        alone[engine] = sum(w for _, w in sample) / t
+    top = curve[-1]
+    return {"curve": curve, "p50_s": top["p50_s"], "p99_s": top["p99_s"], "rate_per_s": top["rate_per_s"],
+            "offered_site_updates_per_s": top["offered_site_updates_per_s"],
+            "served_site_updates_per_s": top["served_site_updates_per_s"],
+            "alone_plain_site_updates_per_s": alone["plain"], "alone_batched_site_updates_per_s": alone["batched"],
+            "alone_sample": f"the stream's first {len(sample)} requests, each run alone through "
+                            "run_temperature_scan, one after another (wall clock, disorder and jackknife included)",
+            "arrival_window_s": args.serve_seconds, "sweep_scale": args.serve_scale,
+            "quantum_sweeps": args.serve_quantum,
+            "note": "request shapes follow the serving configuration (L, p, T, realizations); sweeps are scaled so "
+                    "that the offered load is near what one B200 serves (unscaled, the stream offers ~7.8e12 "
+                    "site-updates/s, far beyond it)"}
 
 
 def main():
@@ -396,25 +477,25 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="resident CTA size (0 = default)")
     ap.add_argument("--e2e-sweeps", type=int, default=200)
     ap.add_argument("--plain-sweeps", type=int, default=200)
-    ap.add_argument("--ref-seconds", type=float, default=3.0)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=1.5, help="CPU seconds per reference-arm step")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--chains", type=int, default=0, help="use only the first N chains (profiling runs)")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' lines")
-    ap.add_argument("--c4-full", action="store_true",
-                    help="also time the whole uneven-size configuration (about 1e6 lattices; slow host setup)")
-    ap.add_argument("--serve-seconds", type=float, default=12.0, help="serving leg arrival window (0 = skip)")
-    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--c2-sweeps", type=int, default=2000)
+    ap.add_argument("--no-c4-full", action="store_true", help="skip the whole uneven-size configuration (1e6 lattices)")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="serving arrival window per rate (0 = skip)")
+    ap.add_argument("--serve-rates", default="5,10,15,20", help="arrival rates of the serving curve (per s)")
     ap.add_argument("--serve-scale", type=float, default=0.004, help="sweeps per request scaled by this factor")
     ap.add_argument("--serve-quantum", type=int, default=10)
+    ap.add_argument("--serve-alone", type=int, default=8, help="requests run alone for the comparison")
     args = ap.parse_args()
 
     L, ps, n_real, temps = workload(args.workload)
-    metric = "L=256 SW sweeps/s batched vs plain on 1 B200 (obs within 2σ); scan p99 latency"
     if args.impl == "reference":
-        return run_reference(args, L, ps, temps, metric)
+        return run_reference(args, L, ps, n_real, temps)
 
     import torch
     import torch.distributed as dist
@@ -477,8 +558,10 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = BYTES_PER_SITE_UPDATE * site_updates_launch / launch_s / 1e9
     kernel = "k_resident_sweeps" if L <= rb._native.resident_max_l() else "k_cluster_sweeps"
-    traffic = profiled_traffic(os.path.join(PROFILES, f"{kernel}_L{L}.txt"))
-    sm_pct = profiled_sm_throughput(os.path.join(PROFILES, f"{kernel}_L{L}.txt"))
+    summary = os.path.join(PROFILES, f"{kernel}_L{L}.txt")
+    traffic = profiled_figure(summary, "dram_bytes_per_launch_scaled")
+    sm_pct = profiled_figure(summary, "sm__throughput (pct of peak)")
+    del cs
 
     # Plain engine: one lattice per launch sequence, same L.
     plain = None
@@ -489,14 +572,7 @@ def main():
         pcs.init_spins(hot=True)
         pcs.run_plain(10)
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        pcs.run_plain(args.plain_sweeps)
-        e1.record(stream)
-        e1.synchronize()
-        pcs.check_status()
-        plain_v = args.plain_sweeps / (e0.elapsed_time(e1) / 1000.0)
+        plain_v = args.plain_sweeps / time_sweeps(pcs, args.plain_sweeps, plain=True)
         plain = {"value": plain_v, "unit": "lattice-sweeps/s", "engine": "plain (global-memory, per-phase launches)",
                  "batched_over_plain": value / world / plain_v}
 
@@ -538,17 +614,16 @@ def main():
 
     configs = None
     if rank == 0 and not args.no_configs:
-        configs = config_lines(rb, dev, args.seed)
-    if rank == 0 and args.c4_full:
+        configs = config_lines(rb, dev, args.seed, args.c2_sweeps)
+    if rank == 0 and not args.no_c4_full:
         configs = dict(configs or {}, c4_full=c4_full_line(rb, dev, args.seed))
     serving = None
     if rank == 0 and args.serve_seconds > 0:
-        serving = serving_leg(rb, dev, args.serve_seconds, args.serve_rate, args.serve_scale, args.seed,
-                              args.serve_quantum)
+        serving = serving_leg(rb, dev, args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(L, temps, ps, seconds=args.cpu_seconds)
+        cpu = cpu_baseline(rb, L, ps, n_real, temps, args.seed, seconds=args.cpu_seconds)
 
     if world > 1:
         dist.barrier()
@@ -556,7 +631,7 @@ def main():
     if rank != 0:
         return
     line = {
-        "metric": metric,
+        "metric": METRIC,
         "value": value,
         "unit": "lattice-sweeps/s",
         "n_gpus": world,
@@ -568,11 +643,9 @@ def main():
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic (seeded +-J disorder from the reference's generator)",
-        "config": {"workload": args.workload, "L": L, "p": ps, "realizations_per_p": n_real,
-                   "temperatures": [float(temps[0]), float(temps[-1]), len(temps)], "chains_per_gpu": n_chains,
-                   "sweeps_per_step": S, "measured": True,
-                   "engine": "resident (batched)" if kernel == "k_resident_sweeps" else "cluster (batched)",
-                   "l2": "flushed between steps (256 MB write)", "parallelism": f"independent chains x{world}"},
+        "config": workload_config(args, L, ps, n_real, temps),
+        "engine": "resident (batched)" if kernel == "k_resident_sweeps" else "cluster (batched)",
+        "chains_per_gpu": n_chains,
         "site_updates_per_s": value * L * L,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",

@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define RBIM_ABI_VERSION 1
+#define RBIM_ABI_VERSION 2
 
 enum {
     RBIM_OK = 0,
@@ -60,7 +60,9 @@ enum {
 enum {
     RBIM_STATUS_FIND_CAP = 1,  /* a union-find walk exceeded its bound */
     RBIM_STATUS_UNION_CAP = 2, /* a union retried beyond its bound */
-    RBIM_STATUS_BAD_CHAIN = 4  /* a chain descriptor was out of range */
+    RBIM_STATUS_BAD_CHAIN = 4  /* a chain descriptor was out of range: L outside the call's range (or, on the
+                                  plain path, different from the call's L), sweeps_per_bin < 1, n_bins < 0,
+                                  n_therm < 0 or walk_cap < 0; the chain is skipped and left unchanged */
 };
 
 /*
@@ -80,7 +82,12 @@ typedef struct rbim_chain_t {
     int64_t n_bins;        /* measured sweeps are n_therm .. n_therm + n_bins*sweeps_per_bin - 1 */
     int64_t sweeps_per_bin;
     int64_t L;             /* linear size, 3 <= L */
-    int64_t reserved;      /* must be 0 */
+    int64_t walk_cap;      /* 0: the default bounds.  > 0: a test hook that lowers the bound on one
+                              union-find walk from N + 64 steps to walk_cap (and the per-thread loop
+                              bounds to 64 walk_cap), so that a small lattice makes the bounds fire
+                              and the call returns with RBIM_STATUS_FIND_CAP / _UNION_CAP set.  The
+                              resident and plain engines honour it; the cluster engine keeps its own
+                              bounds.  A chain run with a lowered cap has undefined results. */
 } rbim_chain_t;
 
 /*
@@ -91,13 +98,16 @@ typedef struct rbim_chain_t {
  * (reference PRIMITIVES, src/rbim/simulation.py:56-71; per-bin means are the
  * sums divided by sweeps_per_bin).  Sweep calls add into the rows, so the
  * caller zeroes them before the first call.
- * Records (optional): 8 int32 per measured sweep:
- *   E, M, n_clusters, S1, |M_C1|, S2, wrap_x, wrap_y
- * (reference SweepResult, src/rbim/swendsen_wang.py:24-53).
+ * Records (optional): 9 int32 per measured sweep:
+ *   E, M, n_clusters, S1, |M_C1|, S2, |M_C2|, wrap_x, wrap_y
+ * (the fields of the reference's SweepResult, src/rbim/swendsen_wang.py:24-53,
+ * in order; S2 = |M_C2| = 0 when there is one cluster).  |M_C2| is computed
+ * only for chains whose records are written.  Among clusters of equal size
+ * the one with the smaller smallest site ranks first.
  */
 #define RBIM_ACC_INT 12
 #define RBIM_ACC_F64 2
-#define RBIM_REC_LEN 8
+#define RBIM_REC_LEN 9
 
 /* Message of the calling thread's last failed call ("" if none). */
 const char *rbim_last_error(void);
@@ -214,14 +224,20 @@ int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const
  * rbim_sweeps_plain, minus workspace and workspace_bytes: the scratch is one
  * static device array of 2.25 MiB per device inside the library, enough for
  * L <= RBIM_NOALLOC_MAX_L.  Larger L is rejected with RBIM_ERR_UNSUPPORTED
- * and a message naming the limit.  Nothing is allocated, by the library or
- * by any library it calls.
+ * and a message naming the limit.  The call itself allocates nothing, and
+ * calls no allocating routine of any library (see the set-up note below for
+ * the one-time placement of the array).
  *
- * The first call on each device (the device current on the calling thread)
- * does the set-up: it looks up the array's device address with
- * cudaGetSymbolAddress and caches it; make that first call before any stream
- * capture begins.  Nothing has to start at zero: the call initialises every
- * part of the scratch it reads.  The scratch is shared by all calls on a
+ * Every call looks up the array's device address on the calling thread's
+ * current device with cudaGetSymbolAddress (cheap once the library's device
+ * code is loaded, and never stale across a cudaDeviceReset).  The driver
+ * places the array when it loads the library's device code on a device --
+ * with lazy module loading, the default, that happens at the first call into
+ * the library on that device (this one, rbim_init_spins or any other) -- and
+ * that load needs about 2.25 MiB of free device memory: make the first call
+ * on each device before a pooling allocator reserves the device's memory,
+ * and before any stream capture begins.  Nothing has to start at zero: the
+ * call initialises every part of the scratch it reads.  The scratch is shared by all calls on a
  * device, so two calls that overlap on the device (different streams, or
  * different host threads, without ordering between them) race on it and give
  * wrong results; order them on one stream or serialise them.

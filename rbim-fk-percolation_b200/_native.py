@@ -31,7 +31,7 @@ __all__ = [
 
 ACC_INT = 12
 ACC_F64 = 2
-REC_LEN = 8
+REC_LEN = 9
 
 #: numpy mirror of ``rbim_chain_t`` (96 bytes, every field 8 bytes).
 CHAIN_DTYPE = np.dtype(
@@ -47,7 +47,7 @@ CHAIN_DTYPE = np.dtype(
         ("n_bins", "<i8"),
         ("sweeps_per_bin", "<i8"),
         ("L", "<i8"),
-        ("reserved", "<i8"),
+        ("walk_cap", "<i8"),
     ]
 )
 assert CHAIN_DTYPE.itemsize == 96

@@ -108,21 +108,34 @@ def _report(name: str, temperatures: np.ndarray, curves: Dict[int, np.ndarray]) 
     return est
 
 
-def validate_pure_ising(args) -> Tuple[Optional[float], Optional[float]]:
+def pure_ising_curves(sizes: Sequence[int], temperatures: np.ndarray, sweeps: int, bins: int, seed: int,
+                      chunk: int = 500, verbose: bool = False):
+    """Binder-cumulant and wrap_y curves of the pure model (p = 0, one realization) for every size.
+
+    Same scans as the reference's ``validate_pure_ising.py:99-113`` (seed ``seed + L`` per size), run as
+    concurrent requests of one scan server.  Returns ``(binder, wrapping)``, dicts keyed by L.
+    """
     rb = _package()
-    temperatures = np.linspace(args.t_min, args.t_max, args.n_temps)
-    print(f"exact T_c = {TC_EXACT:.6f}")
-    print(f"sizes {args.sizes}, {args.n_temps} temperatures in [{args.t_min}, {args.t_max}], {args.sweeps} sweeps")
     binder, wrapping = {}, {}
-    with rb.ScanServer(quantum=args.chunk) as server:
+    with rb.ScanServer(quantum=chunk) as server:
         futs = {L: server.submit(rb.ScanRequest(L=L, p=0.0, temperatures=temperatures, n_realizations=1,
-                                                n_sweeps=args.sweeps, n_bins=args.bins, seed=args.seed + L))
-                for L in args.sizes}
+                                                n_sweeps=sweeps, n_bins=bins, seed=seed + L))
+                for L in sizes}
         for L, f in futs.items():
             res = f.result()
             binder[L] = res["observables"]["binder"]["value"]
             wrapping[L] = res["observables"]["wrap_y"]["value"]
-            print(f"  L={L:3d} done")
+            if verbose:
+                print(f"  L={L:3d} done")
+    return binder, wrapping
+
+
+def validate_pure_ising(args) -> Tuple[Optional[float], Optional[float]]:
+    temperatures = np.linspace(args.t_min, args.t_max, args.n_temps)
+    print(f"exact T_c = {TC_EXACT:.6f}")
+    print(f"sizes {args.sizes}, {args.n_temps} temperatures in [{args.t_min}, {args.t_max}], {args.sweeps} sweeps")
+    binder, wrapping = pure_ising_curves(args.sizes, temperatures, args.sweeps, args.bins, args.seed, args.chunk,
+                                         verbose=True)
     b = _report("Binder cumulant", temperatures, binder)
     w = _report("FK wrapping probability", temperatures, wrapping)
     if b is not None and w is not None:

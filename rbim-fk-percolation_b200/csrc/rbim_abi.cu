@@ -310,8 +310,14 @@ int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const
 //
 // The plain engine's workspace for L <= RBIM_NOALLOC_MAX_L lives in one
 // file-scope device array, so the entry point needs no caller workspace and
-// allocates nothing.  Its device address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current.
+// allocates nothing itself.  Its device address is looked up on every call
+// with cudaGetSymbolAddress, with the calling thread's current device
+// current: the lookup is cheap once the module is loaded, and a cached
+// address would go stale if the primary context were torn down and created
+// again (cudaDeviceReset reloads the module at a new address).  The driver
+// places the array when it loads this module on a device -- with lazy module
+// loading, at the first call into the library on that device -- and that load
+// needs about 2.25 MiB of free device memory.
 // The scratch needs no clearing by anyone: every part of it the sweep reads
 // is written earlier in the same call (k_plain_begin zeroes the seam plane
 // and the scalar block, the phases rewrite the union-find words and the bit
@@ -323,32 +329,18 @@ namespace {
 constexpr int64_t kNoAllocMaxL = RBIM_NOALLOC_MAX_L;
 // 2.25 MiB; rbim::plain_workspace_bytes(512) is 2,295,296 bytes.
 constexpr size_t kNoAllocScratchBytes = size_t(2304) * 1024;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch on the current device (set-up on first use).
+// Device address of the scratch on the current device.
 int noalloc_scratch(void **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_check(e, "rbim_sweeps_plain_noalloc: cudaGetDevice");
-    if (dev < 0 || dev >= kNoAllocMaxDevices)
-        return fail(RBIM_ERR_UNSUPPORTED, "rbim_sweeps_plain_noalloc: device index %d >= %d", dev,
-                    kNoAllocMaxDevices);
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_check(e, "rbim_sweeps_plain_noalloc: cudaGetSymbolAddress");
-        if (!p || ((uintptr_t)p & 255u) != 0)
-            return fail(RBIM_ERR_CUDA, "rbim_sweeps_plain_noalloc: scratch address %p is not 256-byte aligned", p);
-        g_noalloc_addr[dev] = p;
-    }
-    *out = g_noalloc_addr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_check(e, "rbim_sweeps_plain_noalloc: cudaGetSymbolAddress");
+    if (!p || ((uintptr_t)p & 255u) != 0)
+        return fail(RBIM_ERR_CUDA, "rbim_sweeps_plain_noalloc: scratch address %p is not 256-byte aligned", p);
+    *out = p;
     return RBIM_OK;
 }
 

@@ -143,13 +143,13 @@ namespace {
 struct CRed {
     unsigned long long k1[32], k2[32];
     uint32_t unsat[32], downs[32], ncl[32];
-    int mcw[32];
+    int mcw[32], mcw2[32];
     // This CTA's partial results, read by rank 0 through DSMEM.
     unsigned long long p_k1, p_k2;
     uint32_t p_unsat, p_downs, p_ncl;
-    int p_wrap, p_mc;
+    int p_wrap, p_mc, p_mc2;
     // Rank 0's combined results, read by the other CTAs.
-    uint32_t g1, ncl_total;
+    uint32_t g1, g2, ncl_total;
     // Per chain / per sweep state.
     int item, wrap, err;
     uint32_t front, tile_end;
@@ -249,71 +249,67 @@ __device__ __forceinline__ void tile_activate(const Ctx &x, const Tile &tl, cons
     const uint32_t chunk0 = tl.b >> 7;
     const uint32_t last = tl.Tc - 1u;
     const bool end_is_row_end = ((tl.b + tl.Tc) % tl.L) == 0u;
-    for (uint32_t c0 = warp; c0 < nchunks; c0 += 2u * nwarps) {
-        uint32_t sh[2], sv[2], re[2], wq[2];
-        U4 r[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t c = c0 + k * nwarps;
-            wq[k] = 4u * c + lane;
-            sh[k] = sv[k] = re[k] = 0;
-            if (lane < 4u && wq[k] < g.NW) {
-                const uint32_t v = g.valid(wq[k]);
-                re[k] = tile_row_end(tl, wq[k], v);
-                const uint32_t s = t.S[wq[k]];
-                sh[k] = ~(s ^ extract_nowrap(t.S, (wq[k] << 5) + tl.L) ^ gJH[wq[k]]) & v;
-                sv[k] = ~(s ^ tile_ynext(t.S, wq[k], re[k], tl.L, front) ^ gJV[wq[k]]) & v;
-            }
-            r[k] = philox_block(rng.key, 32u * (chunk0 + c) + lane, rng.sweep, kStreamBond);
+    // Groups of G consecutive words, as in phase_activate_bonds: lane j forms
+    // the satisfied masks of word j, then the warp draws the group's chunks
+    // two at a time and lane j keeps the ballots of its own word.
+    uint32_t G = 32u;
+    while (G > 4u && G * nwarps > g.NW) G >>= 1;
+    const uint32_t ngroups = (g.NW + G - 1u) / G;
+    const uint32_t my_chunk = lane >> 2, my_s = lane & 3u;
+    for (uint32_t grp = warp; grp < ngroups; grp += nwarps) {
+        const uint32_t w = grp * G + lane;
+        const bool mine = lane < G && w < g.NW;
+        uint32_t sh = 0, sv = 0, re = 0;
+        if (mine) {
+            const uint32_t v = g.valid(w);
+            re = tile_row_end(tl, w, v);
+            const uint32_t s = t.S[w];
+            sh = ~(s ^ extract_nowrap(t.S, (w << 5) + tl.L) ^ gJH[w]) & v;
+            sv = ~(s ^ tile_ynext(t.S, w, re, tl.L, front) ^ gJV[w]) & v;
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t c = c0 + k * nwarps;
-            // Acceptance of this lane's eight draws, before the satisfied
-            // masks: bit 0 horizontal (low half), bit 16 vertical (high half).
-            uint32_t acc[4], eq = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const uint32_t w = u4_word(r[k], s);
-                const uint32_t lo = w & 0xFFFFu, hi = w >> 16;
-                acc[s] = ((rng.thr_all || lo < rng.thr_hi) ? 1u : 0u) | ((rng.thr_all || hi < rng.thr_hi) ? 0x10000u : 0u);
-                eq |= ((lo == rng.thr_hi) ? 1u : 0u) << (2 * s);
-                eq |= ((hi == rng.thr_hi) ? 2u : 0u) << (2 * s);
-            }
-            if (!rng.thr_all && __any_sync(0xFFFFFFFFu, eq != 0u)) {
-                const U4 q = philox_block(rng.key, 32u * (chunk0 + c) + lane, rng.sweep, kStreamBondLow);
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const uint32_t w = u4_word(q, s);
-                    if ((eq >> (2 * s)) & 1u) acc[s] |= ((w & 0xFFFFu) < rng.thr_lo) ? 1u : 0u;
-                    if ((eq >> (2 * s)) & 2u) acc[s] |= ((w >> 16) < rng.thr_lo) ? 0x10000u : 0u;
-                }
-            }
-            uint32_t oh = 0, ov = 0;
+        const uint32_t c0 = grp * (G >> 2);
+        const uint32_t nch = min(G >> 2, nchunks - c0);
+        uint32_t oh = 0, ov = 0;
+        for (uint32_t k = 0; k < nch; k += 2u) {
+            const bool two = k + 1u < nch;
+            const uint32_t b0 = 32u * (chunk0 + c0 + k) + lane, b1 = b0 + 32u;
+            const U4 r0 = philox_block(rng.key, b0, rng.sweep, kStreamBond);
+            U4 r1{};
+            if (two) r1 = philox_block(rng.key, b1, rng.sweep, kStreamBond);
+            const uint32_t a0 = accept_block(rng, r0, b0);
+            const uint32_t a1 = two ? accept_block(rng, r1, b1) : 0u;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, acc[s] & 1u);
-                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, acc[s] >> 16);
-                if (lane == (uint32_t)s) {
-                    oh = bh & sh[k];
-                    ov = bv & sv[k];
+                const uint32_t bh0 = __ballot_sync(0xFFFFFFFFu, (a0 >> s) & 1u);
+                const uint32_t bv0 = __ballot_sync(0xFFFFFFFFu, (a0 >> (4 + s)) & 1u);
+                const uint32_t bh1 = __ballot_sync(0xFFFFFFFFu, (a1 >> s) & 1u);
+                const uint32_t bv1 = __ballot_sync(0xFFFFFFFFu, (a1 >> (4 + s)) & 1u);
+                if (my_s == (uint32_t)s) {
+                    if (my_chunk == k) {
+                        oh = bh0;
+                        ov = bv0;
+                    } else if (my_chunk == k + 1u) {
+                        oh = bh1;
+                        ov = bv1;
+                    }
                 }
             }
-            if (lane < 4u && wq[k] < g.NW) {
-                const uint32_t w = wq[k];
-                uint32_t keep = ov & ~re[k];
-                if (w == (last >> 5) && !end_is_row_end) {
-                    const uint32_t eb = 1u << (last & 31u);
-                    red.tile_end = (keep & eb) ? 1u : 0u;
-                    keep &= ~eb;
-                }
-                t.OH[w] = oh;
-                t.OV[w] = keep;
-                if (ov & re[k]) {
-                    const uint32_t bit = __ffs(re[k]) - 1u;
-                    const uint32_t row = (tl.b + (w << 5) + bit + 1u) / tl.L - 1u - tl.x0;
-                    atomicOr(x.YS + (row >> 5), 1u << (row & 31u));
-                }
+        }
+        if (mine) {
+            oh &= sh;
+            ov &= sv;
+            uint32_t keep = ov & ~re;
+            if (w == (last >> 5) && !end_is_row_end) {
+                const uint32_t eb = 1u << (last & 31u);
+                red.tile_end = (keep & eb) ? 1u : 0u;
+                keep &= ~eb;
+            }
+            t.OH[w] = oh;
+            t.OV[w] = keep;
+            if (ov & re) {
+                const uint32_t bit = __ffs(re) - 1u;
+                const uint32_t row = (tl.b + (w << 5) + bit + 1u) / tl.L - 1u - tl.x0;
+                atomicOr(x.YS + (row >> 5), 1u << (row & 31u));
             }
         }
     }
@@ -626,7 +622,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
         __syncthreads();
         const rbim_chain_t &ch = red.ch;
         const bool bad = ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 ||
-                         ch.n_therm < 0 || !cluster_tiles_ok((uint32_t)ch.L, C, kCap) ||
+                         ch.n_therm < 0 || ch.walk_cap < 0 || !cluster_tiles_ok((uint32_t)ch.L, C, kCap) ||
                          cluster_tile_size((uint32_t)(ch.L * ch.L), C) > ly.t_max;
         if (bad) {
             if (tid == 0 && c == 0) atomicOr(status, kErrBadChain);
@@ -834,32 +830,46 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 }
                 if (lane == 0) {
                     red.g1 = 0xFFFFFFFFu - (uint32_t)(a1 & 0xFFFFFFFFull);
+                    red.g2 = 0xFFFFFFFFu - (uint32_t)(a2 & 0xFFFFFFFFull);
                     red.ncl_total = sn;
                     rec[0] = 2ll * (long long)su - 2ll * (long long)tl.N;
                     rec[1] = (long long)tl.N - 2ll * (long long)sd;
                     rec[2] = sn;
                     rec[3] = (long long)(a1 >> 32);
                     rec[5] = (long long)(a2 >> 32);
-                    rec[6] = wr & 1;
-                    rec[7] = (wr >> 1) & 1;
+                    rec[7] = wr & 1;
+                    rec[8] = (wr >> 1) & 1;
                 }
             }
             cl.sync();  // rank 0's results are visible
             if (tid == 0 && c != 0) {
                 const CRed *o = cl.map_shared_rank(&red, 0);
                 red.g1 = o->g1;
+                red.g2 = o->g2;
                 red.ncl_total = o->ncl_total;
             }
             __syncthreads();
-            const uint32_t g1 = red.g1;
+            const uint32_t g1 = red.g1, g2 = red.g2;
             const bool many = red.ncl_total > 1u;
+            // |M_C2| only when the chain's records are written (the bin sums
+            // do not use it).
+            const bool second = records && ch.rec_off >= 0;
             if (many) {
-                // Tile roots of the largest cluster, marked in OH.
-                for (uint32_t w = tid; w < t.g.NW; w += NT) t.OH[w] = 0u;
+                // Tile roots of the largest cluster, marked in OH, and with
+                // `second` those of the second largest in OV (whose node
+                // marks are no longer needed).
+                for (uint32_t w = tid; w < t.g.NW; w += NT) {
+                    t.OH[w] = 0u;
+                    if (second) t.OV[w] = 0u;
+                }
                 __syncthreads();
                 if (tid == 0 && g1 >= tl.b && g1 < tl.b + tl.Tc) {
                     const uint32_t m = g1 - tl.b;
                     atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
+                }
+                if (second && tid == 0 && g2 >= tl.b && g2 < tl.b + tl.Tc) {
+                    const uint32_t m = g2 - tl.b;
+                    atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
                 }
                 for (uint32_t k = tid; k < x.hs; k += NT) {
                     if (x.HK[k] == kEmptyKey) continue;
@@ -869,36 +879,57 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                     if (gr == g1) {
                         const uint32_t m = x.HK[k];
                         atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
+                    } else if (second && gr == g2) {
+                        const uint32_t m = x.HK[k];
+                        atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
                     }
                 }
                 __syncthreads();
-                int mc = 0;
+                int mc = 0, mc2 = 0;
                 for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
                     const uint32_t n = (w << 5) + lane;
-                    bool in = false;
+                    bool in = false, in2 = false;
                     if (n < t.g.N) {
                         const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
                         in = (t.OH[r >> 5] >> (r & 31u)) & 1u;
+                        if (second) in2 = (t.OV[r >> 5] >> (r & 31u)) & 1u;
                     }
+                    const uint32_t sw = t.S[w];
                     const uint32_t mm = __ballot_sync(0xFFFFFFFFu, in);
-                    if (lane == 0) mc += (int)__popc(mm) - 2 * (int)__popc(mm & t.S[w]);
+                    if (lane == 0) mc += (int)__popc(mm) - 2 * (int)__popc(mm & sw);
+                    if (second) {
+                        const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, in2);
+                        if (lane == 0) mc2 += (int)__popc(m2) - 2 * (int)__popc(m2 & sw);
+                    }
                 }
-                if (lane == 0) red.mcw[warp] = mc;
+                if (lane == 0) {
+                    red.mcw[warp] = mc;
+                    red.mcw2[warp] = mc2;
+                }
                 __syncthreads();
                 if (tid == 0) {
-                    int s = 0;
-                    for (uint32_t i = 0; i < nwarps; ++i) s += red.mcw[i];
+                    int s = 0, s2 = 0;
+                    for (uint32_t i = 0; i < nwarps; ++i) {
+                        s += red.mcw[i];
+                        s2 += red.mcw2[i];
+                    }
                     red.p_mc = s;
+                    red.p_mc2 = s2;
                 }
             }
             cl.sync();  // M_C partials are visible
             if (c == 0 && tid == 0) {
-                long long mc_total = rec[1];
+                long long mc_total = rec[1], mc2_total = 0;
                 if (many) {
                     mc_total = 0;
-                    for (uint32_t i = 0; i < C; ++i) mc_total += cl.map_shared_rank(&red, i)->p_mc;
+                    for (uint32_t i = 0; i < C; ++i) {
+                        const CRed *o = cl.map_shared_rank(&red, i);
+                        mc_total += o->p_mc;
+                        mc2_total += o->p_mc2;
+                    }
                 }
                 rec[4] = mc_total < 0 ? -mc_total : mc_total;
+                rec[6] = mc2_total < 0 ? -mc2_total : mc2_total;
                 const long long idx = (long long)(sweep - (uint64_t)ch.n_therm);
                 const long long bin = idx / ch.sweeps_per_bin;
                 if (bin != red.cur_bin) {
@@ -908,8 +939,8 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                     red.acc.load(acc_i + (ch.acc_off + bin) * kAccInt, acc_f + (ch.acc_off + bin) * kAccF64);
                     red.cur_bin = bin;
                 }
-                red.acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[6], (int)rec[7]);
-                if (records && ch.rec_off >= 0) {
+                red.acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[7], (int)rec[8]);
+                if (second) {
                     int32_t *row = records + (ch.rec_off + idx) * kRecLen;
 #pragma unroll
                     for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];

@@ -354,12 +354,13 @@ __device__ __forceinline__ void warp_top2(K &k1, K &k2)
 
 // ---------------------------------------------------------------------------
 // Per-sweep record and primitive accumulation.
-// Record: E, M, n_clusters, S1, |M_C1|, S2, wrap_x, wrap_y.
+// Record: E, M, n_clusters, S1, |M_C1|, S2, |M_C2|, wrap_x, wrap_y (the fields
+// of the reference's SweepResult, src/rbim/swendsen_wang.py:24-53, in order).
 // Integer sums per bin: E, E^2, M, |M|, M^2, S1, |M_C1|, S2, n_clusters,
 //                       wrap_x, wrap_y, wrap_any            (int64)
 // Floating sums per bin: M^4, |M_C1|/S1                     (double)
 // ---------------------------------------------------------------------------
-constexpr int kRecLen = 8;
+constexpr int kRecLen = 9;
 constexpr int kAccInt = 12;
 constexpr int kAccF64 = 2;
 

@@ -117,7 +117,7 @@ __device__ __forceinline__ void phase_union_open(const Lat<Word16> &t, uint32_t 
     uint32_t item = tid, pending = 0, base = 0;
     uint32_t xa = 0, xb = 0;
     bool fetch = true;
-    const uint32_t cap = 64u * g.N + 4096u;
+    const uint32_t cap = 64u * t.cap;  // 64 walks of t.cap steps (64 N + 4096 by default)
     uint32_t it = 0;
     RBIM_PROF_ONLY(uint32_t n_bonds = 0; uint32_t n_fails = 0);
     for (;; ++it) {
@@ -207,7 +207,7 @@ __device__ __forceinline__ uint32_t phase_roots_flat(const Lat<Word16> &t, uint3
     bool a1 = a0 && next_head(t, sl, nthreads, item, pending, base, h1);
     x0 = h0;
     x1 = h1;
-    const uint32_t cap = 64u * g.N + 4096u;
+    const uint32_t cap = 64u * t.cap;  // 64 walks of t.cap steps (64 N + 4096 by default)
     for (uint32_t it = 0; a0 || a1; ++it) {
         if (it >= cap) {
             atomicOr(t.err, kErrFindCap);

@@ -32,7 +32,7 @@ struct Lat {
     const uint32_t *RE;    // row-end masks per word (Geom::row_end), or null to compute them
     int *wrap;             // bit 0 wrap_x, bit 1 wrap_y
     int *err;
-    uint32_t cap;
+    uint32_t cap;          // bound on the steps of one walk (N + 64 unless a chain's walk_cap lowers it)
     __device__ __forceinline__ uint32_t row_end(uint32_t w) const { return RE ? RE[w] : g.row_end(w); }
 };
 
@@ -64,83 +64,107 @@ __device__ __forceinline__ uint32_t bond_decide(const SweepRng &rng, uint32_t u)
     return u == rng.thr_hi ? 2u : 0u;
 }
 
-// (a) Bond activation.  Items are 128-site chunks (four plane words); lane i
-// of the warp owning chunk c draws Philox block 32c + i, whose word s holds
-// the 16-bit draws of the horizontal (low half) and vertical (high half) bond
-// of site 128c + 32s + i, i.e. bit i of the chunk's word s, so that each
-// ballot is one word of the occupied-bond planes.  SEAMV must be zero on
-// entry.
+// Acceptance of one lane's Philox block of bond draws: bit s of the result
+// accepts the horizontal bond of word s (low half of word s of the block),
+// bit 4 + s the vertical one (high half); satisfied masks are applied later.
+// A 16-bit draw equal to thr >> 16 defers to the low half drawn from stream
+// 3 (probability 2^-16 per bond), fetched when any lane of the warp needs it.
+__device__ __forceinline__ uint32_t accept_block(const SweepRng &rng, const U4 &r, uint32_t block)
+{
+    uint32_t acc = 0, eq = 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const uint32_t w = u4_word(r, s);
+        const uint32_t lo = w & 0xFFFFu, hi = w >> 16;
+        acc |= ((rng.thr_all || lo < rng.thr_hi) ? 1u : 0u) << s;
+        acc |= ((rng.thr_all || hi < rng.thr_hi) ? 1u : 0u) << (4 + s);
+        eq |= ((lo == rng.thr_hi) ? 1u : 0u) << s;
+        eq |= ((hi == rng.thr_hi) ? 1u : 0u) << (4 + s);
+    }
+    if (!rng.thr_all && __any_sync(0xFFFFFFFFu, eq != 0u)) {
+        const U4 q = philox_block(rng.key, block, rng.sweep, kStreamBondLow);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t w = u4_word(q, s);
+            if ((eq >> s) & 1u) acc |= ((w & 0xFFFFu) < rng.thr_lo ? 1u : 0u) << s;
+            if ((eq >> (4 + s)) & 1u) acc |= ((w >> 16) < rng.thr_lo ? 1u : 0u) << (4 + s);
+        }
+    }
+    return acc;
+}
+
+// (a) Bond activation.  A 128-site chunk is four plane words; lane i of the
+// warp handling chunk c draws Philox block 32c + i, whose word s holds the
+// 16-bit draws of the horizontal (low half) and vertical (high half) bond of
+// site 128c + 32s + i, i.e. bit i of the chunk's word s, so that each ballot
+// is one word of the occupied-bond planes.  A warp takes a group of G
+// consecutive words (G = 32, eight chunks, while every warp still gets a
+// group): lane j first forms the satisfied masks of word j of the group --
+// every lane busy, coalesced loads -- then the warp draws the group's chunks
+// two at a time, and lane j keeps the ballots of its own word.  SEAMV must be
+// zero on entry.
 template <class WT>
 __device__ __forceinline__ void phase_activate_bonds(const Lat<WT> &t, const SweepRng &rng, uint32_t warp,
                                                      uint32_t nwarps)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const Geom &g = t.g;
-    const uint32_t nchunks = (g.N + 127u) >> 7;
     Plane S{t.S};
-    // Two chunks per iteration (c and c + nwarps): two independent Philox
-    // evaluations per lane.
-    for (uint32_t c0 = warp; c0 < nchunks; c0 += 2u * nwarps) {
-        uint32_t sh[2], sv[2], re[2], wq[2];
-        U4 r[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t c = c0 + k * nwarps;
-            // Lanes 0..3 form the satisfied masks of the chunk's four words.
-            wq[k] = 4u * c + lane;
-            sh[k] = sv[k] = re[k] = 0;
-            if (lane < 4u && wq[k] < g.NW) {
-                re[k] = t.row_end(wq[k]);
-                const uint32_t v = g.valid(wq[k]);
-                const uint32_t s = S(wq[k]);
-                sh[k] = ~(s ^ xnext_word(S, wq[k], g) ^ t.JH[wq[k]]) & v;
-                sv[k] = ~(s ^ ynext_word(S, wq[k], g, re[k]) ^ t.JV[wq[k]]) & v;
-            }
-            r[k] = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBond);
+    uint32_t G = 32u;
+    while (G > 4u && G * nwarps > g.NW) G >>= 1;
+    const uint32_t ngroups = (g.NW + G - 1u) / G;
+    const uint32_t nchunks = (g.NW + 3u) >> 2;
+    const uint32_t my_chunk = lane >> 2, my_s = lane & 3u;
+    for (uint32_t grp = warp; grp < ngroups; grp += nwarps) {
+        const uint32_t w = grp * G + lane;
+        const bool mine = lane < G && w < g.NW;
+        uint32_t sh = 0, sv = 0, re = 0;
+        if (mine) {
+            re = t.row_end(w);
+            const uint32_t v = g.valid(w);
+            const uint32_t s = S(w);
+            sh = ~(s ^ xnext_word(S, w, g) ^ t.JH[w]) & v;
+            sv = ~(s ^ ynext_word(S, w, g, re) ^ t.JV[w]) & v;
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t c = c0 + k * nwarps;
-            // Acceptance of this lane's eight draws, before the satisfied
-            // masks: bit 0 horizontal (low half), bit 16 vertical (high half).
-            uint32_t acc[4], eq = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const uint32_t w = u4_word(r[k], s);
-                const uint32_t lo = w & 0xFFFFu, hi = w >> 16;
-                acc[s] = ((rng.thr_all || lo < rng.thr_hi) ? 1u : 0u) | ((rng.thr_all || hi < rng.thr_hi) ? 0x10000u : 0u);
-                eq |= ((lo == rng.thr_hi) ? 1u : 0u) << (2 * s);
-                eq |= ((hi == rng.thr_hi) ? 2u : 0u) << (2 * s);
-            }
-            if (!rng.thr_all && __any_sync(0xFFFFFFFFu, eq != 0u)) {
-                const U4 q = philox_block(rng.key, 32u * c + lane, rng.sweep, kStreamBondLow);
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const uint32_t w = u4_word(q, s);
-                    if ((eq >> (2 * s)) & 1u) acc[s] |= ((w & 0xFFFFu) < rng.thr_lo) ? 1u : 0u;
-                    if ((eq >> (2 * s)) & 2u) acc[s] |= ((w >> 16) < rng.thr_lo) ? 0x10000u : 0u;
-                }
-            }
-            uint32_t oh = 0, ov = 0;
+        const uint32_t c0 = grp * (G >> 2);
+        const uint32_t nch = min(G >> 2, nchunks - c0);
+        uint32_t oh = 0, ov = 0;
+        // Two chunks per iteration: two independent Philox evaluations per lane.
+        for (uint32_t k = 0; k < nch; k += 2u) {
+            const bool two = k + 1u < nch;
+            const U4 r0 = philox_block(rng.key, 32u * (c0 + k) + lane, rng.sweep, kStreamBond);
+            U4 r1{};
+            if (two) r1 = philox_block(rng.key, 32u * (c0 + k + 1u) + lane, rng.sweep, kStreamBond);
+            const uint32_t a0 = accept_block(rng, r0, 32u * (c0 + k) + lane);
+            const uint32_t a1 = two ? accept_block(rng, r1, 32u * (c0 + k + 1u) + lane) : 0u;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const uint32_t bh = __ballot_sync(0xFFFFFFFFu, acc[s] & 1u);
-                const uint32_t bv = __ballot_sync(0xFFFFFFFFu, acc[s] >> 16);
-                if (lane == (uint32_t)s) {
-                    oh = bh & sh[k];
-                    ov = bv & sv[k];
+                const uint32_t bh0 = __ballot_sync(0xFFFFFFFFu, (a0 >> s) & 1u);
+                const uint32_t bv0 = __ballot_sync(0xFFFFFFFFu, (a0 >> (4 + s)) & 1u);
+                const uint32_t bh1 = __ballot_sync(0xFFFFFFFFu, (a1 >> s) & 1u);
+                const uint32_t bv1 = __ballot_sync(0xFFFFFFFFu, (a1 >> (4 + s)) & 1u);
+                if (my_s == (uint32_t)s) {
+                    if (my_chunk == k) {
+                        oh = bh0;
+                        ov = bv0;
+                    } else if (my_chunk == k + 1u) {
+                        oh = bh1;
+                        ov = bv1;
+                    }
                 }
             }
-            if (lane < 4u && wq[k] < g.NW) {
-                t.OH[wq[k]] = oh;
-                t.OV[wq[k]] = ov & ~re[k];
-                uint32_t seam = ov & re[k];
-                while (seam) {
-                    const uint32_t b = __ffs(seam) - 1u;
-                    seam &= seam - 1u;
-                    const uint32_t x = ((wq[k] << 5) + b) / g.L;
-                    atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
-                }
+        }
+        if (mine) {
+            oh &= sh;
+            ov &= sv;
+            t.OH[w] = oh;
+            t.OV[w] = ov & ~re;
+            uint32_t seam = ov & re;
+            while (seam) {
+                const uint32_t b = __ffs(seam) - 1u;
+                seam &= seam - 1u;
+                const uint32_t x = ((w << 5) + b) / g.L;
+                atomicOr(t.SEAMV + (x >> 5), 1u << (x & 31u));
             }
         }
     }
@@ -333,7 +357,7 @@ __device__ __forceinline__ void phase_union(const Lat<WT> &t, uint32_t tid, uint
     Walk<WT> a{}, b{};
     int ex = 0;
     bool fetch = true;
-    const unsigned long long cap = 64ull * g.N + 4096ull;
+    const unsigned long long cap = 64ull * t.cap;  // 64 walks of t.cap steps (64 N + 4096 by default)
     for (unsigned long long it = 0;; ++it) {
         if (it >= cap) {
             atomicOr(t.err, kErrUnionCap);
@@ -432,7 +456,7 @@ __device__ __forceinline__ uint32_t phase_roots(const Lat<WT> &t, uint32_t tid, 
     bool a0 = next_head_of(t, sl, nthreads, item, pending, base, h0);
     bool a1 = a0 && next_head_of(t, sl, nthreads, item, pending, base, h1);
     uint32_t x0 = h0, x1 = h1;
-    const unsigned long long cap = 64ull * g.N + 4096ull;
+    const unsigned long long cap = 64ull * t.cap;  // 64 walks of t.cap steps (64 N + 4096 by default)
     for (unsigned long long it = 0; a0 || a1; ++it) {
         if (it >= cap) {
             atomicOr(t.err, kErrFindCap);

@@ -6,6 +6,7 @@
 // enqueued (or captured in a CUDA graph) without host round trips; kernels of
 // a chain that has finished its run return immediately.
 #include <algorithm>
+#include <mutex>
 
 #include "rbim_internal.h"
 #include "rbim_phases.cuh"
@@ -24,7 +25,9 @@ struct PlainScratch {
     unsigned long long unsat;
     unsigned long long downs;
     long long mc;
+    long long mc2;
     unsigned long long g1;
+    unsigned long long g2;
     unsigned long long s1;
     unsigned long long s2;
     unsigned int done1;  // CTAs of k_plain_measure1 finished this sweep
@@ -44,16 +47,27 @@ struct PlainSizes {
     size_t uf, plane, seam, sc, top2, total;
 };
 
+// Grid of the plain kernels on the current device: 4 CTAs per SM, cached per
+// device (a process may drive devices with different SM counts).
 int plain_grid()
 {
-    static int g = 0;
-    if (!g) {
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        g = std::max(1, sms) * 4;
+    constexpr int kDevices = 64;
+    static int grid[kDevices];
+    static std::mutex mu;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+        cudaGetLastError();
+        return 148 * 4;
     }
-    return g;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!grid[dev]) {
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return 148 * 4;
+        }
+        grid[dev] = std::max(1, sms) * 4;
+    }
+    return grid[dev];
 }
 
 constexpr int kMaxPlainGrid = 4096;
@@ -96,6 +110,7 @@ PlainWs plain_ws(void *base, int64_t L)
 }
 
 struct PlainArgs {
+    int64_t L;  // the size the workspace was sized for; the descriptor must agree
     rbim_chain_t *chain;
     uint32_t *spin_pool;
     const uint32_t *coupling_pool;
@@ -106,9 +121,20 @@ struct PlainArgs {
     PlainWs ws;
 };
 
-// Phase of the chain's current sweep: 0 = finished, 1 = thermalisation, 2 = measured.
-__device__ __forceinline__ int chain_phase(const rbim_chain_t *c)
+// A descriptor the plain kernels can run: the size the launch (and its
+// workspace) was made for, and a well-formed run layout.
+__device__ __forceinline__ bool chain_ok(const PlainArgs &a)
 {
+    const rbim_chain_t *c = a.chain;
+    return c->L == a.L && c->sweeps_per_bin >= 1 && c->n_bins >= 0 && c->n_therm >= 0 && c->walk_cap >= 0;
+}
+
+// Phase of the chain's current sweep: 0 = finished (or a descriptor that
+// fails chain_ok), 1 = thermalisation, 2 = measured.
+__device__ __forceinline__ int chain_phase(const PlainArgs &a)
+{
+    if (!chain_ok(a)) return 0;
+    const rbim_chain_t *c = a.chain;
     const uint64_t s = *((volatile const uint64_t *)&c->sweep);
     const uint64_t end = (uint64_t)c->n_therm + (uint64_t)c->n_bins * (uint64_t)c->sweeps_per_bin;
     if (s >= end) return 0;
@@ -132,7 +158,9 @@ __device__ __forceinline__ Lat<Word64> plain_lat(const PlainArgs &a)
     t.RE = nullptr;
     t.wrap = &a.ws.sc->wrap;
     t.err = &a.ws.sc->err;
-    t.cap = t.g.N + 64u;
+    // A descriptor's walk_cap > 0 lowers the walk bound (a test hook).
+    const int64_t wc = a.chain->walk_cap;
+    t.cap = (wc > 0 && wc < (int64_t)(t.g.N + 64u)) ? (uint32_t)wc : t.g.N + 64u;
     return t;
 }
 
@@ -143,7 +171,12 @@ __device__ __forceinline__ uint32_t gnthreads() { return gridDim.x * blockDim.x;
 
 __global__ void k_plain_begin(PlainArgs a)
 {
-    const uint32_t L = (uint32_t)a.chain->L;
+    if (!chain_ok(a)) {
+        // Every later kernel of the call returns at once for this descriptor.
+        if (gtid() == 0) atomicOr(a.status, kErrBadChain);
+        return;
+    }
+    const uint32_t L = (uint32_t)a.L;
     for (uint32_t i = gtid(); i < (L + 31u) / 32u; i += gnthreads()) a.ws.SEAMV[i] = 0u;
     if (gtid() == 0) {
         PlainScratch z{};
@@ -151,9 +184,9 @@ __global__ void k_plain_begin(PlainArgs a)
     }
 }
 
-__global__ void __launch_bounds__(kPlainThreads) k_plain_activate(PlainArgs a)
+__global__ void __launch_bounds__(kPlainThreads, 4) k_plain_activate(PlainArgs a)
 {
-    if (!chain_phase(a.chain)) return;
+    if (!chain_phase(a)) return;
     const Lat<Word64> t = plain_lat(a);
     const SweepRng rng = make_rng(a.chain->key, a.chain->sweep, a.chain->thr);
     phase_activate<Word64>(t, rng, gwarp(), gnwarps(), gtid(), gnthreads());
@@ -162,7 +195,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_activate(PlainArgs a)
 // Run heads; also clears the ROOT plane for the root walks that follow.
 __global__ void __launch_bounds__(kPlainThreads) k_plain_heads(PlainArgs a)
 {
-    if (!chain_phase(a.chain)) return;
+    if (!chain_phase(a)) return;
     const Lat<Word64> t = plain_lat(a);
     for (uint32_t w = gtid(); w < t.g.NW; w += gnthreads()) t.ROOT[w] = 0u;
     phase_heads<Word64>(t, gwarp(), gnwarps());
@@ -170,13 +203,13 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_heads(PlainArgs a)
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_union(PlainArgs a)
 {
-    if (!chain_phase(a.chain)) return;
+    if (!chain_phase(a)) return;
     phase_union<Word64>(plain_lat(a), gtid(), gnthreads());
 }
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_roots(PlainArgs a)
 {
-    if (!chain_phase(a.chain)) return;
+    if (!chain_phase(a)) return;
     const Lat<Word64> t = plain_lat(a);
     uint32_t nr = phase_roots<Word64>(t, gtid(), gnthreads());
 #pragma unroll
@@ -186,7 +219,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_roots(PlainArgs a)
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_finalize(PlainArgs a)
 {
-    const int ph = chain_phase(a.chain);
+    const int ph = chain_phase(a);
     if (!ph) return;
     const Lat<Word64> t = plain_lat(a);
     phase_sites<Word64>(t, gwarp(), gnwarps(), true, ph == 2);
@@ -195,7 +228,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_finalize(PlainArgs a)
 
 __global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
 {
-    if (chain_phase(a.chain) != 2) return;
+    if (chain_phase(a) != 2) return;
     const Lat<Word64> t = plain_lat(a);
     uint32_t unsat = 0, downs = 0;
     measure_energy(t, gtid(), gnthreads(), unsat, downs);
@@ -263,6 +296,7 @@ __global__ void __launch_bounds__(kPlainThreads) k_plain_measure1(PlainArgs a)
         if (lane == 0) {
             PlainScratch *sc = a.ws.sc;
             sc->g1 = 0xFFFFFFFFull - (b1 & 0xFFFFFFFFull);
+            sc->g2 = 0xFFFFFFFFull - (b2 & 0xFFFFFFFFull);
             sc->s1 = b1 >> 32;
             sc->s2 = b2 >> 32;
         }
@@ -281,13 +315,15 @@ __device__ void plain_end(const PlainArgs &a, int ph)
         const long long N = c->L * c->L;
         const long long M = N - 2ll * (long long)sc->downs;
         const long long ncl = sc->nroots;
-        long long s1 = (long long)sc->s1, s2 = (long long)sc->s2, mc = sc->mc;
+        long long s1 = (long long)sc->s1, s2 = (long long)sc->s2, mc = sc->mc, mc2 = sc->mc2;
         if (ncl == 1) {
             s1 = N;
             s2 = 0;
             mc = M;
+            mc2 = 0;
         }
         if (mc < 0) mc = -mc;
+        if (mc2 < 0) mc2 = -mc2;
         const long long E = 2ll * (long long)sc->unsat - 2ll * N;
         const int wrap = sc->wrap;
         const int wx = wrap & 1, wy = (wrap >> 1) & 1;
@@ -305,8 +341,9 @@ __device__ void plain_end(const PlainArgs &a, int ph)
             row[3] = (int32_t)s1;
             row[4] = (int32_t)mc;
             row[5] = (int32_t)s2;
-            row[6] = wx;
-            row[7] = wy;
+            row[6] = (int32_t)mc2;
+            row[7] = wx;
+            row[8] = wy;
         }
     }
     const int err = sc->err;
@@ -317,25 +354,33 @@ __device__ void plain_end(const PlainArgs &a, int ph)
 }
 
 // Magnetisation of the largest cluster (measured sweeps with more than one
-// cluster), then, in the last CTA to finish, the end of the sweep: every CTA
-// adds its share, fences and takes a ticket, so the last ticket sees all
-// shares.  Thermalisation sweeps run only the ticket and the end.
+// cluster) and, when the chain's records are written, of the second largest;
+// then, in the last CTA to finish, the end of the sweep: every CTA adds its
+// share, fences and takes a ticket, so the last ticket sees all shares.
+// Thermalisation sweeps run only the ticket and the end.
 __global__ void __launch_bounds__(kPlainThreads) k_plain_measure3(PlainArgs a)
 {
-    const int ph = chain_phase(a.chain);
+    const int ph = chain_phase(a);
     if (!ph) return;
     if (ph == 2 && a.ws.sc->nroots > 1) {
         const Lat<Word64> t = plain_lat(a);
-        const uint32_t g1 = (uint32_t)a.ws.sc->g1;
+        const uint32_t g1 = (uint32_t)a.ws.sc->g1, g2 = (uint32_t)a.ws.sc->g2;
+        const bool second = a.records && a.chain->rec_off >= 0;
         const uint32_t lane = threadIdx.x & 31u;
-        int mc = 0;
+        int mc = 0, mc2 = 0;
         for (uint32_t w = gwarp(); w < t.g.NW; w += gnwarps()) {
             const uint32_t n = (w << 5) + lane;
-            const bool in = n < t.g.N && Word64::parent(t.uf.ldc(n)) == g1;
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, in);
-            if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & t.S[w]);
+            const uint32_t r = n < t.g.N ? Word64::parent(t.uf.ldc(n)) : 0xFFFFFFFFu;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, r == g1);
+            const uint32_t sw = t.S[w];
+            if (lane == 0) mc += (int)__popc(m) - 2 * (int)__popc(m & sw);
+            if (second) {
+                const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, r == g2);
+                if (lane == 0) mc2 += (int)__popc(m2) - 2 * (int)__popc(m2 & sw);
+            }
         }
         if (lane == 0 && mc) atomicAdd((unsigned long long *)&a.ws.sc->mc, (unsigned long long)(long long)mc);
+        if (lane == 0 && mc2) atomicAdd((unsigned long long *)&a.ws.sc->mc2, (unsigned long long)(long long)mc2);
     }
     // Every thread fences its own adds before the CTA's ticket is taken.
     __threadfence();
@@ -475,7 +520,7 @@ cudaError_t launch_plain_sweeps(rbim_chain_t *chain, uint32_t *spin_pool, const 
                                 long long *acc_i, double *acc_f, int32_t *records, int n_sweeps, int *status,
                                 void *workspace, int64_t L, cudaStream_t stream)
 {
-    PlainArgs a{chain, spin_pool, coupling_pool, acc_i, acc_f, records, status, plain_ws(workspace, L)};
+    PlainArgs a{L, chain, spin_pool, coupling_pool, acc_i, acc_f, records, status, plain_ws(workspace, L)};
     const int grid = std::min(plain_grid(), kMaxPlainGrid);
     k_plain_begin<<<1, 256, 0, stream>>>(a);
     for (int s = 0; s < n_sweeps; ++s) {

@@ -171,9 +171,9 @@ template <int NT>
 struct Red {
     uint32_t k1[NT / 32], k2[NT / 32];
     uint32_t unsat[NT / 32], downs[NT / 32], roots[NT / 32];
-    int mc[NT / 32];
+    int mc[NT / 32], mc2[NT / 32];
     int item, wrap, err;
-    uint32_t ncl, g1, s1, s2, unsat_t, downs_t;
+    uint32_t ncl, g1, g2, s1, s2, unsat_t, downs_t;
     // State of the chain being processed; only thread 0 updates it.
     Acc acc;
     long long cur_bin;
@@ -194,8 +194,12 @@ struct Res {
     uint32_t hs, hs_log2;
 };
 
+// walk_cap > 0 lowers the per-walk bound (and with it the per-thread loop
+// bounds, 64 walks' worth) from N + 64 steps to walk_cap: the chain
+// descriptor's test hook that makes the bounds fire on a small lattice.
 template <int NT>
-__device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayout &ly, uint32_t L, Red<NT> &red)
+__device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayout &ly, uint32_t L, Red<NT> &red,
+                                        int64_t walk_cap = 0)
 {
     Res r;
     Lat<Word16> &t = r.t;
@@ -213,7 +217,7 @@ __device__ __forceinline__ Res make_res(unsigned char *smem, const ResidentLayou
     t.SEAMV = (uint32_t *)(smem + ly.off_SEAMV);
     t.wrap = &red.wrap;
     t.err = &red.err;
-    t.cap = t.g.N + 64u;
+    t.cap = (walk_cap > 0 && walk_cap < (int64_t)(t.g.N + 64u)) ? (uint32_t)walk_cap : t.g.N + 64u;
     r.HK = (uint32_t *)(smem + ly.off_HK);
     r.HW = (uint32_t *)(smem + ly.off_HW);
     r.hs = ly.hs;
@@ -356,12 +360,12 @@ __device__ __forceinline__ uint32_t resident_label(const Res &r, bool flip)
 }
 
 // Measurement of one sweep after resident_label: energy, magnetization,
-// n_clusters, S1, S2, |M_C1| (reference sw_sweep,
-// src/rbim/swendsen_wang.py:146-172).  Ends with a barrier.  Thread 0 returns
-// the record in rec.
+// n_clusters, S1, S2, |M_C1| and, with `second` (records requested), |M_C2|
+// (reference sw_sweep, src/rbim/swendsen_wang.py:146-172).  Ends with a
+// barrier.  Thread 0 returns the record in rec.
 template <int NT>
 __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, uint32_t nroots_warp,
-                                                 long long rec[kRecLen])
+                                                 long long rec[kRecLen], bool second)
 {
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     constexpr uint32_t nwarps = NT / 32;
@@ -434,14 +438,15 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             warp_top2(a1, a2);
             if (lane == 0) {
                 red.g1 = 0xFFFFu - (a1 & 0xFFFFu);
+                red.g2 = 0xFFFFu - (a2 & 0xFFFFu);
                 red.s1 = a1 >> 16;
                 red.s2 = a2 >> 16;
             }
         }
         __syncthreads();
         RBIM_PHASE_MARK(8);
-        const uint32_t g1 = red.g1;
-        int mc = 0;
+        const uint32_t g1 = red.g1, g2 = red.g2;
+        int mc = 0, mc2 = 0;
         // Two words per iteration keep two load chains in flight.
         for (uint32_t w0 = warp; w0 < g.NW; w0 += 2u * nwarps) {
             const uint32_t w1 = w0 + nwarps;
@@ -449,16 +454,25 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
             const uint32_t rt0 = t.ROOT[w0], rt1 = w1 < g.NW ? t.ROOT[w1] : 0u;
             const bool ok0 = n0 < g.N, ok1 = n1 < g.N;
             const uint32_t p0 = ok0 ? (uint32_t)u16[n0] : 0u, p1 = ok1 ? (uint32_t)u16[n1] : 0u;
-            const bool in0 = ok0 && (((rt0 >> lane) & 1u) ? n0 == g1 : p0 == g1);
-            const bool in1 = ok1 && (((rt1 >> lane) & 1u) ? n1 == g1 : p1 == g1);
-            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, in0);
-            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, in1);
+            const uint32_t r0 = ((rt0 >> lane) & 1u) ? n0 : p0, r1 = ((rt1 >> lane) & 1u) ? n1 : p1;
+            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, ok0 && r0 == g1);
+            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, ok1 && r1 == g1);
+            const uint32_t s0 = t.S[w0], s1 = w1 < g.NW ? t.S[w1] : 0u;
             if (lane == 0) {
-                mc += (int)__popc(m0) - 2 * (int)__popc(m0 & t.S[w0]);
-                if (w1 < g.NW) mc += (int)__popc(m1) - 2 * (int)__popc(m1 & t.S[w1]);
+                mc += (int)__popc(m0) - 2 * (int)__popc(m0 & s0);
+                mc += (int)__popc(m1) - 2 * (int)__popc(m1 & s1);
+            }
+            if (second) {
+                const uint32_t q0 = __ballot_sync(0xFFFFFFFFu, ok0 && r0 == g2);
+                const uint32_t q1 = __ballot_sync(0xFFFFFFFFu, ok1 && r1 == g2);
+                if (lane == 0) mc2 += (int)__popc(q0) - 2 * (int)__popc(q0 & s0) + (int)__popc(q1) -
+                                      2 * (int)__popc(q1 & s1);
             }
         }
-        if (lane == 0) red.mc[warp] = mc;
+        if (lane == 0) {
+            red.mc[warp] = mc;
+            red.mc2[warp] = mc2;
+        }
         __syncthreads();
         RBIM_PHASE_MARK(9);
     } else if (tid == 0) {
@@ -469,10 +483,13 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
     }
     const long long M = (long long)g.N - 2ll * (long long)red.downs_t;
     if (tid == 0) {
-        long long mc_total = M;
+        long long mc_total = M, mc2_total = 0;
         if (ncl > 1) {
             mc_total = 0;
-            for (uint32_t i = 0; i < nwarps; ++i) mc_total += red.mc[i];
+            for (uint32_t i = 0; i < nwarps; ++i) {
+                mc_total += red.mc[i];
+                mc2_total += red.mc2[i];
+            }
         }
         rec[0] = 2ll * (long long)red.unsat_t - 2ll * (long long)g.N;
         rec[1] = M;
@@ -480,8 +497,9 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         rec[3] = red.s1;
         rec[4] = mc_total < 0 ? -mc_total : mc_total;
         rec[5] = red.s2;
-        rec[6] = red.wrap & 1;
-        rec[7] = (red.wrap >> 1) & 1;
+        rec[6] = mc2_total < 0 ? -mc2_total : mc2_total;
+        rec[7] = red.wrap & 1;
+        rec[8] = (red.wrap >> 1) & 1;
     }
     __syncthreads();
 }
@@ -514,13 +532,14 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
         const int item = red.item;
         if (item >= n_chains) break;
         const rbim_chain_t &ch = red.ch;
-        if (ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 || ch.n_therm < 0) {
+        if (ch.L < 3 || ch.L > (int64_t)ly.l_max || ch.sweeps_per_bin < 1 || ch.n_bins < 0 || ch.n_therm < 0 ||
+            ch.walk_cap < 0) {
             if (tid == 0) atomicOr(status, kErrBadChain);
             __syncthreads();
             continue;
         }
         const uint32_t L = (uint32_t)ch.L;
-        const Res res = make_res<NT>(smem, ly, L, red);
+        const Res res = make_res<NT>(smem, ly, L, red, ch.walk_cap);
         const Lat<Word16> &t = res.t;
         const Geom g = t.g;
         const uint32_t nwp = (g.NW + 3u) & ~3u;
@@ -553,7 +572,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
             const uint32_t nr = resident_label<NT>(res, true);
             if (measure) {
                 long long rec[kRecLen];
-                resident_measure<NT>(res, red, nr, rec);
+                const bool want_rec = records && ch.rec_off >= 0;
+                resident_measure<NT>(res, red, nr, rec, want_rec);
                 if (tid == 0) {
                     const long long idx = (long long)(sweep - (uint64_t)ch.n_therm);
                     const long long bin = idx / ch.sweeps_per_bin;
@@ -566,8 +586,8 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT>::value)
                         red.acc.load(acc_i + (ch.acc_off + bin) * kAccInt, acc_f + (ch.acc_off + bin) * kAccF64);
                         red.cur_bin = bin;
                     }
-                    red.acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[6], (int)rec[7]);
-                    if (records && ch.rec_off >= 0) {
+                    red.acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[7], (int)rec[8]);
+                    if (want_rec) {
                         int32_t *row = records + (ch.rec_off + idx) * kRecLen;
 #pragma unroll
                         for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];

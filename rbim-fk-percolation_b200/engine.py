@@ -13,6 +13,7 @@ the stream; every computation is a call into ``librbim_sm100.so``.
 from __future__ import annotations
 
 import ctypes
+import threading
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
@@ -21,7 +22,8 @@ import numpy as np
 from . import _native
 from .packing import threshold, unpack_spins, words_for
 
-__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_MIN_L", "auto_engine"]
+__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_MIN_L", "auto_engine", "Launch",
+           "launch_buckets"]
 
 #: A set of one lattice runs on the plain engine under ``engine="auto"`` when
 #: its L exceeds this (measured on B200: below it one resident CTA is faster).
@@ -45,6 +47,92 @@ def _package():
     import importlib
 
     return importlib.import_module(__package__)
+
+
+#: Bytes of workspace per concurrent bucket launch: one work-queue counter.
+QUEUE_SLOT = 256
+
+_streams_lock = threading.Lock()
+_side_streams = {}
+
+
+def _side(device, n: int):
+    """``n`` side streams of ``device``, created once per process and reused."""
+    torch = _torch()
+    with _streams_lock:
+        pool = _side_streams.setdefault(device.index, [])
+        while len(pool) < n:
+            pool.append(torch.cuda.Stream(device))
+        return pool[:n]
+
+
+@dataclass
+class Launch:
+    """One on-chip launch of a call: ``kind`` 0 resident (``rbim_sweeps_batched``) or 1 cluster
+    (``rbim_sweeps_clustered``), over ``count`` consecutive descriptors at device address ``chains``."""
+
+    kind: int
+    chains: int
+    count: int
+    l_max: int
+    threads: int = 0
+
+
+def launch_buckets(lib, device, stream, launches: Sequence[Launch], *, spin_pool: int, coupling_pool: int,
+                   acc_int: int, acc_f64: int, records: Optional[int], n_sweeps: int, status: int, workspace: int,
+                   workspace_bytes: int, concurrent: bool = True) -> None:
+    """Advance every bucket of a call by ``n_sweeps``, the buckets running concurrently.
+
+    Each launch is a persistent grid that pulls lattices from its own work
+    queue (slot ``i`` of ``QUEUE_SLOT`` bytes of the workspace) and exits when
+    the queue is empty; with several buckets they are issued on side streams
+    forked from ``stream`` and joined back into it, so that a bucket's CTAs
+    take the SMs that another bucket's tail leaves idle instead of waiting for
+    the whole previous launch.  Cluster launches go first (a cluster needs
+    whole SMs), then resident ones from the largest CTA size to the smallest,
+    which fill what is left.  Results do not depend on the order: every chain
+    is independent.  ``concurrent=False`` issues them one after another on
+    ``stream`` instead.  Pointers are device addresses (ints); ``stream`` is a
+    ``torch.cuda.Stream``.
+    """
+    torch = _torch()
+    launches = list(launches)
+    if not launches or n_sweeps <= 0:
+        return
+    if workspace_bytes < QUEUE_SLOT * len(launches):
+        raise ValueError(f"workspace of {workspace_bytes} bytes is too small for {len(launches)} launches")
+    order = sorted(launches, key=lambda b: (b.kind != 1, -b.threads, -b.count))
+    p = ctypes.c_void_p
+    rec = p(records) if records else None
+
+    def issue(b: Launch, i: int, s) -> None:
+        sp = p(s.cuda_stream)
+        ws = p(workspace + QUEUE_SLOT * i)
+        if b.kind == 0:
+            rc = lib.rbim_sweeps_batched(p(b.chains), b.count, b.l_max, p(spin_pool), p(coupling_pool), p(acc_int),
+                                         p(acc_f64), rec, int(n_sweeps), int(b.threads), p(status), ws, QUEUE_SLOT, sp)
+            _native.check(rc, "rbim_sweeps_batched")
+        elif b.kind == 1:
+            rc = lib.rbim_sweeps_clustered(p(b.chains), b.count, b.l_max, p(spin_pool), p(coupling_pool), p(acc_int),
+                                           p(acc_f64), rec, int(n_sweeps), p(status), ws, QUEUE_SLOT, sp)
+            _native.check(rc, "rbim_sweeps_clustered")
+        else:
+            raise ValueError(f"launch kind {b.kind} is not an on-chip engine")
+
+    if len(order) == 1 or not concurrent:
+        for i, b in enumerate(order):
+            issue(b, i, stream)
+        return
+    fork = torch.cuda.Event()
+    fork.record(stream)
+    side = _side(device, len(order))
+    for i, (b, s) in enumerate(zip(order, side)):
+        s.wait_event(fork)
+        issue(b, i, s)
+    for s in side:
+        done = torch.cuda.Event()
+        done.record(s)
+        stream.wait_event(done)
 
 
 def require_cuda(device=None):
@@ -222,12 +310,20 @@ class ChainSet:
         src = _torch().from_numpy(np.ascontiguousarray(words, dtype="<u4").view(np.int32))
         self.spin_pool[self.spin_off[i]: self.spin_off[i] + nw].copy_(src)
 
-    def set_sweep(self, i: int, sweep: int) -> None:
-        """Set chain ``i``'s sweep counter (host and device copies)."""
+    def set_descriptor_field(self, i: int, name: str, value: int) -> None:
+        """Write one field of chain ``i``'s ``rbim_chain_t`` (host and device copies).
+
+        No check is made beyond the field's type: this is how a caller sets
+        ``walk_cap`` or, in tests, a descriptor the kernels must reject.
+        """
         k = int(self.slot[i])
-        self.desc_host["sweep"][k] = sweep
+        self.desc_host[name][k] = value
         row = _torch().from_numpy(self.desc_host[k: k + 1].view(np.uint8).copy())
         self.chains[96 * k: 96 * (k + 1)].copy_(row)
+
+    def set_sweep(self, i: int, sweep: int) -> None:
+        """Set chain ``i``'s sweep counter (host and device copies)."""
+        self.set_descriptor_field(i, "sweep", sweep)
         self._sweep_host[i] = min(sweep, self.n_total[i])
 
     def spin_words(self, i: int) -> np.ndarray:
@@ -238,42 +334,46 @@ class ChainSet:
         return unpack_spins(self.spin_words(i), self.specs[i].L)
 
     # -- sweeps ------------------------------------------------------------
-    def run_batched(self, n_sweeps: int, threads: int = 0) -> None:
+    def run_batched(self, n_sweeps: int, threads: int = 0, concurrent: bool = True) -> None:
         """Advance every chain by up to ``n_sweeps`` sweeps.
 
         Chains with L up to ``rbim_resident_max_l()`` run on the resident
-        engine (one lattice per CTA, one launch per power-of-two size class),
-        larger ones up to ``rbim_cluster_max_l()`` on the cluster engine (one
-        lattice per thread-block cluster, one launch per cluster size), and
-        any larger still on the plain engine.  ``threads`` fixes the resident
+        engine (one lattice per CTA, one launch per CTA size class), larger
+        ones up to ``rbim_cluster_max_l()`` on the cluster engine (one lattice
+        per thread-block cluster, one launch per cluster plan), and any larger
+        still on the plain engine.  The on-chip launches of one call run
+        concurrently (:func:`launch_buckets`; ``concurrent=False`` issues them
+        one after another).  ``threads`` fixes the resident
         CTA size; 0 takes the autotuner's choice when it is enabled
         (``autotune.enable()``), else the library's rule.
         """
-        self._run_batched_fixed(n_sweeps, threads, tuned=threads == 0)
+        self._run_batched_fixed(n_sweeps, threads, tuned=threads == 0, concurrent=concurrent)
 
-    def _run_batched_fixed(self, n_sweeps: int, threads: int, tuned: bool = False) -> None:
+    def _run_batched_fixed(self, n_sweeps: int, threads: int, tuned: bool = False, concurrent: bool = True) -> None:
         if n_sweeps <= 0:
             return
         from . import autotune
-        nbytes = int(self.lib.rbim_batched_workspace_bytes())
-        ws = self._workspace(nbytes)
-        recs = self._ptr(self.records) if self.records is not None else None
-        with _torch().cuda.device(self.device):
-            for kind, first, count, l_max in self.buckets:
-                ptr = ctypes.c_void_p(self.chains.data_ptr() + 96 * first)
-                if kind == 0:
-                    nt = autotune.tuned_threads(l_max, self.device) if tuned else threads
-                    rc = self.lib.rbim_sweeps_batched(
-                        ptr, count, l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
-                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps), int(nt),
-                        self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
-                    _native.check(rc, "rbim_sweeps_batched")
-                elif kind == 1:
-                    rc = self.lib.rbim_sweeps_clustered(
-                        ptr, count, l_max, self._ptr(self.spin_pool), self._ptr(self.coupling_pool),
-                        self._ptr(self.acc_int), self._ptr(self.acc_f64), recs, int(n_sweeps),
-                        self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
-                    _native.check(rc, "rbim_sweeps_clustered")
+        torch = _torch()
+        launches = []
+        for kind, first, count, l_max in self.buckets:
+            if kind == 2:
+                continue
+            nt = 0
+            if kind == 0:
+                nt = autotune.tuned_threads(l_max, self.device) if tuned else threads
+                nt = nt or int(self.lib.rbim_resident_threads(l_max))
+            else:
+                nt = int(self.lib.rbim_cluster_threads(l_max))
+            launches.append(Launch(kind, self.chains.data_ptr() + 96 * first, count, l_max, nt))
+        if launches:
+            ws = self._workspace(QUEUE_SLOT * len(launches))
+            with torch.cuda.device(self.device):
+                launch_buckets(self.lib, self.device, torch.cuda.current_stream(self.device), launches,
+                               spin_pool=self.spin_pool.data_ptr(), coupling_pool=self.coupling_pool.data_ptr(),
+                               acc_int=self.acc_int.data_ptr(), acc_f64=self.acc_f64.data_ptr(),
+                               records=self.records.data_ptr() if self.records is not None else None,
+                               n_sweeps=n_sweeps, status=self.status.data_ptr(), workspace=ws.data_ptr(),
+                               workspace_bytes=ws.numel(), concurrent=concurrent)
         if self.plain_only:
             self.run_plain(n_sweeps, self.plain_only)
             done = np.ones(self.n, dtype=bool)

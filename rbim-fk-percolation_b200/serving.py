@@ -34,7 +34,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _native, autotune
-from .engine import _torch, require_cuda
+from .engine import QUEUE_SLOT, Launch, _torch, launch_buckets, require_cuda
 from .packing import pack_couplings, threshold, words_for
 from .simulation import ScanPlan, assemble_scan, plan_temperature_scan
 
@@ -188,8 +188,8 @@ class ScanServer:
             self.desc_host = torch.zeros(96 * max(self.max_chains, 1), dtype=torch.uint8).pin_memory()
             self._desc_copied = torch.cuda.Event()
             self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
-            self.queue_ws = torch.zeros(int(self.lib.rbim_batched_workspace_bytes()), dtype=torch.uint8,
-                                        device=self.device)
+            # One work-queue counter per concurrent bucket launch.
+            self.queue_ws = torch.zeros(QUEUE_SLOT * 64, dtype=torch.uint8, device=self.device)
         self._plain_ws = None
         self._planner = ThreadPoolExecutor(max_workers=2, thread_name_prefix="rbim-scan-plan")
         self._inbox: "queue.Queue[_Pending]" = queue.Queue()
@@ -369,11 +369,11 @@ class ScanServer:
         host[:] = allc.view(np.uint8)
         n = len(allc)
         st = ctypes.c_void_p(self.status.data_ptr())
-        qw = ctypes.c_void_p(self.queue_ws.data_ptr())
         with torch.cuda.stream(self.stream):
             self.desc_dev[: 96 * n].copy_(self.desc_host[: 96 * n], non_blocking=True)
             self._desc_copied.record(self.stream)
             first = 0
+            on_chip, plain = [], []
             for key in keys:
                 group = buckets[key]
                 count = sum(len(a.desc) for a in group)
@@ -381,27 +381,32 @@ class ScanServer:
                 base = self.desc_dev.data_ptr() + 96 * first
                 if key[0] == 0:
                     nt = self.threads or autotune.tuned_threads(l_max, self.device)
-                    rc = self.lib.rbim_sweeps_batched(ctypes.c_void_p(base), count, l_max, pool, pool, ai, af, None,
-                                                      self.quantum, nt, st, qw, self.queue_ws.numel(), sp)
-                    _native.check(rc, "rbim_sweeps_batched")
-                    self.launches += 1
+                    nt = nt or int(self.lib.rbim_resident_threads(l_max))
+                    on_chip.append(Launch(0, base, count, l_max, nt))
                 elif key[0] == 1:
-                    rc = self.lib.rbim_sweeps_clustered(ctypes.c_void_p(base), count, l_max, pool, pool, ai, af,
-                                                        None, self.quantum, st, qw, self.queue_ws.numel(), sp)
-                    _native.check(rc, "rbim_sweeps_clustered")
-                    self.launches += 1
+                    on_chip.append(Launch(1, base, count, l_max, int(self.lib.rbim_cluster_threads(l_max))))
                 else:
-                    need = int(self.lib.rbim_plain_workspace_bytes(l_max))
-                    if self._plain_ws is None or self._plain_ws.numel() < need:
-                        self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
-                    for k in range(count):
-                        rc = self.lib.rbim_sweeps_plain(int(allc["L"][first + k]), ctypes.c_void_p(base + 96 * k),
-                                                        pool, pool, ai, af, None, self.quantum, st,
-                                                        ctypes.c_void_p(self._plain_ws.data_ptr()),
-                                                        self._plain_ws.numel(), sp)
-                        _native.check(rc, "rbim_sweeps_plain")
-                        self.launches += 1
+                    plain += [(int(allc["L"][first + k]), base + 96 * k) for k in range(count)]
                 first += count
+            # The on-chip buckets run concurrently, each with its own queue
+            # counter; lattices only the plain engine takes follow on the
+            # server stream.
+            launch_buckets(self.lib, self.device, self.stream, on_chip, spin_pool=self.word_pool.data_ptr(),
+                           coupling_pool=self.word_pool.data_ptr(), acc_int=self.acc_int.data_ptr(),
+                           acc_f64=self.acc_f64.data_ptr(), records=None, n_sweeps=self.quantum,
+                           status=self.status.data_ptr(), workspace=self.queue_ws.data_ptr(),
+                           workspace_bytes=self.queue_ws.numel())
+            self.launches += len(on_chip)
+            if plain:
+                need = max(int(self.lib.rbim_plain_workspace_bytes(L)) for L, _ in plain)
+                if self._plain_ws is None or self._plain_ws.numel() < need:
+                    self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+                for L, ptr in plain:
+                    rc = self.lib.rbim_sweeps_plain(L, ctypes.c_void_p(ptr), pool, pool, ai, af, None, self.quantum,
+                                                    st, ctypes.c_void_p(self._plain_ws.data_ptr()),
+                                                    self._plain_ws.numel(), sp)
+                    _native.check(rc, "rbim_sweeps_plain")
+                    self.launches += 1
         finished = []
         for a in live:
             a.done = min(a.n_total, a.done + self.quantum)

@@ -102,8 +102,8 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
     if not measure:
         return None
     rec = cs.chain_records(0)[0]
-    wx = bool(rec[6]) if measure_percolation else None
-    wy = bool(rec[7]) if measure_percolation else None
+    wx = bool(rec[7]) if measure_percolation else None
+    wy = bool(rec[8]) if measure_percolation else None
     return SweepResult(energy=float(rec[0]), magnetization=float(rec[1]), n_clusters=int(rec[2]),
                        largest_size=int(rec[3]), largest_abs_magnetization=float(rec[4]), second_size=int(rec[5]),
-                       second_abs_magnetization=float("nan"), wraps_x=wx, wraps_y=wy)
+                       second_abs_magnetization=float(rec[6]), wraps_x=wx, wraps_y=wy)

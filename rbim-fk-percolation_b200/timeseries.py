@@ -5,7 +5,7 @@ at a time through ``sw_sweep`` and keeps the raw series of the energy, the
 largest cluster's size and magnetization, their ratio and ``wrap_y``
 (``measure_autocorrelation.py:69-90``).  Here every (temperature,
 realization) chain of a scan runs in one device batch with per-sweep records
-(8 int32 per sweep, written by the sweep kernels), and only the records come
+(9 int32 per sweep, written by the sweep kernels), and only the records come
 back; the series and the autocorrelation estimate are formed on the host.
 """
 
@@ -25,8 +25,8 @@ __all__ = ["TRACKED", "SERIES", "collect_series", "integrated_autocorrelation"]
 TRACKED = ("energy", "largest_size", "largest_abs_mag", "mag_ratio", "wrap_y")
 
 #: Every series available from the records, in record order plus the ratio.
-SERIES = ("energy", "magnetization", "n_clusters", "largest_size", "largest_abs_mag", "second_size", "wrap_x",
-          "wrap_y", "mag_ratio")
+SERIES = ("energy", "magnetization", "n_clusters", "largest_size", "largest_abs_mag", "second_size",
+          "second_abs_mag", "wrap_x", "wrap_y", "mag_ratio")
 
 
 def collect_series(L: int, p: float, temperatures: Sequence[float], *, n_sweeps: int, n_therm: int,
@@ -51,7 +51,7 @@ def collect_series(L: int, p: float, temperatures: Sequence[float], *, n_sweeps:
     cs.run_to_end(engine="batched", chunk=chunk)
     n_t, n_r = len(plan.temperatures), plan.n_realizations
     rec = cs.records.cpu().numpy().reshape(n_t, n_r, n_sweeps, -1).astype(np.float64)
-    out = {name: rec[..., i] for i, name in enumerate(SERIES[:8])}
+    out = {name: rec[..., i] for i, name in enumerate(SERIES[:9])}
     largest = out["largest_size"]
     with np.errstate(divide="ignore", invalid="ignore"):
         out["mag_ratio"] = np.where(largest > 0, out["largest_abs_mag"] / np.where(largest > 0, largest, 1.0), 0.0)

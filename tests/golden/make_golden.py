@@ -1,9 +1,10 @@
 """Generate the golden fixtures of this directory by running the reference itself.
 
-Run in a container that has the reference checked out (default
-``/root/reference``, override with ``RBIM_REFERENCE``) and numba installed::
+Run in a container that has the reference checked out and numba installed,
+with ``RBIM_REFERENCE`` naming the reference's checkout (the directory that
+holds its ``src/rbim`` and ``tests``)::
 
-    python tests/golden/make_golden.py [--scan-c1]
+    RBIM_REFERENCE=<path to the reference> python tests/golden/make_golden.py [--scan-c1]
 
 It imports the reference package ``rbim`` from ``<reference>/src`` and the
 spanning-forest winding oracle from ``<reference>/tests/test_wrapping.py``, and
@@ -37,7 +38,9 @@ import time
 
 import numpy as np
 
-REF = os.environ.get("RBIM_REFERENCE", "/root/reference")
+REF = os.environ.get("RBIM_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "src", "rbim")):
+    raise SystemExit("set RBIM_REFERENCE to the reference checkout (the directory holding src/rbim and tests)")
 OUT = os.path.dirname(os.path.abspath(__file__))
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "rbim_numba_cache"))
 sys.path.insert(0, os.path.join(REF, "src"))

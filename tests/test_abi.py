@@ -43,7 +43,7 @@ def test_chain_struct_layout_matches_header(rb):
 
 def test_host_only_queries(rb):
     lib = rb._native.lib()
-    assert lib.rbim_abi_version() == 1
+    assert lib.rbim_abi_version() == 2
     assert lib.rbim_plane_words(3) == 4 and lib.rbim_plane_words(64) == 128
     lmax = lib.rbim_resident_max_l()
     assert 128 <= lmax <= 256

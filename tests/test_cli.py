@@ -104,6 +104,8 @@ def test_time_series_match_oracle_records(rb, orc):
                 assert series["energy"][t, r, i] == rec[0]
                 assert series["largest_size"][t, r, i] == rec[3]
                 assert series["largest_abs_mag"][t, r, i] == rec[4]
+                assert series["second_size"][t, r, i] == rec[5]
+                assert series["second_abs_mag"][t, r, i] == rec[6]
                 assert series["wrap_y"][t, r, i] == rec[8]
                 assert series["mag_ratio"][t, r, i] == pytest.approx(rec[4] / rec[3])
 
@@ -119,3 +121,30 @@ def test_validate_pure_ising_finds_tc(rb):
     tc = 2.0 / np.log(1.0 + np.sqrt(2.0))
     assert b is not None and abs(b - tc) < 0.08
     assert w is not None and abs(w - tc) < 0.08
+
+
+@pytest.mark.gpu
+def test_pure_ising_crossings_drift_to_tc(rb):
+    """The reference's validation (``scripts/validate_pure_ising.py``, ``README.md:146-158``) at its own settings
+    (L = 8, 16, 24; 11 temperatures in [2.15, 2.40]; 8,000 sweeps) and at larger sizes (L = 32, 48, 64) with more
+    sweeps: the Binder and wrap_y crossings of successive size pairs move toward the exact T_c as L grows, the
+    largest pair lands within 0.3 % of it, and the two estimates agree (Coniglio-Klein at p = 0)."""
+    cli = _cli()
+    temps = np.linspace(2.15, 2.40, 11)
+    tc = 2.0 / np.log(1.0 + np.sqrt(2.0))
+    table = {}
+    for sizes, sweeps in (((8, 16, 24), 8000), ((32, 48, 64), 40000)):
+        b, w = cli.pure_ising_curves(sizes, temps, sweeps, 10, 0, chunk=2000)
+        table[sizes] = ({(la, lb): t for la, lb, t in cli.pairwise_crossings(temps, b)},
+                        {(la, lb): t for la, lb, t in cli.pairwise_crossings(temps, w)})
+        print(f"crossings {sizes} {sweeps} sweeps: binder {table[sizes][0]} wrap {table[sizes][1]}")
+    bs, ws = table[(8, 16, 24)]
+    bl, wl = table[(32, 48, 64)]
+    # README.md:154-155 at the reference's settings: Binder 2.2491 / 2.2596 / 2.2627, wrapping 2.2645 / 2.2670 / 2.2683.
+    assert bs[(8, 16)] < bs[(16, 24)] < tc + 0.005
+    assert abs(bs[(8, 16)] - 2.2491) < 0.01 and abs(bs[(16, 24)] - 2.2627) < 0.01
+    assert all(abs(t - tc) < 0.012 for t in ws.values()), ws
+    # Larger sizes: closer still.
+    assert abs(bl[(48, 64)] - tc) < abs(bs[(16, 24)] - tc) + 0.002
+    assert abs(bl[(48, 64)] - tc) < 0.3e-2 * tc and abs(wl[(48, 64)] - tc) < 0.3e-2 * tc
+    assert abs(np.mean(list(bl.values())) - np.mean(list(wl.values()))) < 0.006

@@ -139,15 +139,37 @@ def test_c1_scan_matches_reference(rb):
 
 
 def test_large_lattice_critical_energy(rb):
-    """L = 1024 at p = 0 and T_c: E/N within the run's error of Kaufman's exact value."""
+    """The single-lattice configuration's second run: L = 1024, p = 0 at T_c, 2,000 measured sweeps.
+
+    * E/N within the run's error of Kaufman's exact finite-torus value;
+    * Coniglio-Klein, the reference's P_inf = |m| check (``tests/test_physics.py:110-124``): at T_c both scale
+      as L^(-1/8) and the reference's own scans give P_inf / |m| = 0.998 at L = 32 and 0.997 at L = 64
+      (20,000 and 8,000 sweeps), so they agree to within 0.02 at any L;
+    * |m| L^(1/8) = 1.010 (L = 32) and 1.014 (L = 64) in those reference scans, so finite-size scaling puts
+      |m| at L = 1024 near 1.012 * 1024^(-1/8) = 0.425.
+    """
     L = 1024
     J = rb.couplings_from_disorder(np.ones((L, L), np.int8), np.ones((L, L), np.int8))
-    r = rb.run_single_realization(L, J, onsager.TC_EXACT, n_sweeps=200, n_therm=100, n_bins=10, seed=7,
+    r = rb.run_single_realization(L, J, onsager.TC_EXACT, n_sweeps=2000, n_therm=200, n_bins=20, seed=7,
                                   start="cold")
     e = r.primitives["energy"] / (L * L)
     bins = r.bin_primitives["energy"] / (L * L)
     err = bins.std(ddof=1) / np.sqrt(bins.size)
     exact = onsager.energy_per_site_torus(onsager.TC_EXACT, L)
-    assert abs(e - exact) <= 4 * err + 2e-4, (e, exact, err)
+    assert abs(e - exact) <= 4 * err + 1e-4, (e, exact, err)
     d = rb.derive_observables(r.primitives, onsager.TC_EXACT, L * L)
-    assert 0.0 < d["p_infinity"] < 1.0
+    assert d["p_infinity"] == pytest.approx(d["abs_magnetization"], abs=0.02), d
+    assert d["abs_magnetization"] == pytest.approx(1.012 * L ** (-0.125), abs=0.03), d
+
+
+def test_large_lattice_ordered_phase(rb):
+    """L = 1024, p = 0 at T = 2.0 (reference ``tests/test_physics.py:92-124`` at the single-lattice size):
+    |m| on Onsager's curve (no visible finite-size offset at this L), P_inf = |m|, and the percolating
+    cluster's spins aligned."""
+    L = 1024
+    J = rb.couplings_from_disorder(np.ones((L, L), np.int8), np.ones((L, L), np.int8))
+    r = rb.run_single_realization(L, J, 2.0, n_sweeps=1000, n_therm=200, n_bins=10, seed=2024, start="cold")
+    d = rb.derive_observables(r.primitives, 2.0, L * L)
+    assert d["abs_magnetization"] == pytest.approx(onsager.onsager_magnetization(2.0), abs=0.005), d
+    assert d["p_infinity"] == pytest.approx(d["abs_magnetization"], abs=0.01), d
+    assert d["cluster_magnetization_ratio"] > 0.9

@@ -120,6 +120,28 @@ def test_plain_chain_bit_exact(rb, orc, L):
     _chain(rb, orc, [L] * 2, "plain")
 
 
+@pytest.mark.parametrize("L", [300, 512, 1024, 1500])
+def test_plain_chain_bit_exact_large(rb, orc, L):
+    """The plain engine at the sizes engine="auto" sends to it: every single lattice with L > 128, and every
+    lattice beyond the cluster engine (L > 1024).  p = 0.10 at T = 1.6 (one cluster spans the lattice) and at
+    T_c of the pure model."""
+    _chain(rb, orc, [L, L], "plain", n_therm=2, n_bins=2, spb=2, temps=(1.6, 2.269))
+
+
+def test_plain_records_large(rb, orc):
+    """Per-sweep records of the plain engine at L = 512, |M_C2| included, equal the oracle's sweep by sweep."""
+    L, n_therm, spb = 512, 1, 2
+    cs, specs, J_host = _chain(rb, orc, [L], "plain", n_therm=n_therm, n_bins=2, spb=spb, temps=(2.269,),
+                               records=True)
+    recs = cs.chain_records(0)
+    s = specs[0]
+    spins = orc.initial_spins(L * L, s.key, hot=True)
+    for t in range(n_therm + 2 * spb):
+        r = orc.sw_sweep(L, spins, J_host[0], s.key, rb.packing.threshold(s.beta), t, measure=t >= n_therm)
+        if t >= n_therm:
+            assert tuple(int(v) for v in recs[t - n_therm]) == tuple(int(v) for v in r), t
+
+
 def test_batched_uneven_sizes_one_launch(rb, orc):
     _chain(rb, orc, [32, 48, 64, 96, 128, 5, 17, 200], "batched", n_therm=3, n_bins=2, spb=4)
 
@@ -139,8 +161,7 @@ def test_records_match_oracle_sweeps(rb, orc):
             for t in range(n_therm + 2 * spb):
                 r = orc.sw_sweep(L, spins, J_host[i], s.key, rb.packing.threshold(s.beta), t, measure=t >= n_therm)
                 if t >= n_therm:
-                    want = (r[0], r[1], r[2], r[3], r[4], r[5], r[7], r[8])
-                    assert tuple(int(v) for v in recs[t - n_therm]) == want, (engine, i, t)
+                    assert tuple(int(v) for v in recs[t - n_therm]) == tuple(int(v) for v in r), (engine, i, t)
 
 
 def test_largest_lattice_on_chip_and_beyond(rb, orc):
@@ -158,7 +179,8 @@ def test_cold_start_and_zero_temperature_limit(rb):
     cs.init_spins(hot=False)
     cs.run_batched(10)
     rec = cs.chain_records(0)
-    assert np.all(rec[:, 2] == 1) and np.all(rec[:, 3] == L * L) and np.all(rec[:, 6] == 1) and np.all(rec[:, 7] == 1)
+    assert np.all(rec[:, 2] == 1) and np.all(rec[:, 3] == L * L) and np.all(rec[:, 7] == 1) and np.all(rec[:, 8] == 1)
+    assert np.all(rec[:, 5] == 0) and np.all(rec[:, 6] == 0)
     assert np.all(np.abs(rec[:, 1]) == L * L) and np.all(rec[:, 0] == -2 * L * L)
 
 
@@ -172,8 +194,8 @@ def test_sw_sweep_api_matches_oracle(rb, orc):
         res = rb.sw_sweep(spins, lattice, J, 1 / 1.8, key=77, sweep=t)
         r = orc.sw_sweep(L, ref, J, 77, rb.packing.threshold(1 / 1.8), t, measure=True)
         assert (res.energy, res.magnetization, res.n_clusters, res.largest_size, res.largest_abs_magnetization,
-                res.second_size, res.wraps_x, res.wraps_y) == (r[0], r[1], r[2], r[3], r[4], r[5], bool(r[7]),
-                                                               bool(r[8]))
+                res.second_size, res.second_abs_magnetization, res.wraps_x, res.wraps_y) == (
+                    r[0], r[1], r[2], r[3], r[4], r[5], r[6], bool(r[7]), bool(r[8]))
         assert np.array_equal(spins, ref.astype(np.int64))
 
 

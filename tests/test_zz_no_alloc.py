@@ -5,8 +5,10 @@ caller workspace -- spins, bin sums (the doubles bit for bit), records,
 sweep counters and status -- over two calls in a row, for lattices of
 different sizes sharing the one scratch (a large L before a small one, so
 stale scratch from the large lattice is present), and reject L above its
-limit with a message naming the limit.  This file is collected last so that
-the GPU case also runs after every other test has used the device.
+limit with a message naming the limit.  The comparison does not depend on
+what ran before: the first lattice (L = 512) fills the scratch and the
+smaller ones that follow meet its stale contents, whether the file runs
+alone in a fresh process or after the rest of the suite.
 """
 
 import ctypes
