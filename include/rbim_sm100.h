@@ -201,6 +201,29 @@ int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uin
                           int n_sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream);
 
 /*
+ * Launch plans of the cluster engine, for a tuner.  A plan is the number of
+ * CTAs per cluster (tiles per lattice) and the CTA size (512: tiles of at
+ * most 32768 sites, two CTAs per SM; 1024: at most 65536 sites, one per SM).
+ * rbim_cluster_plans writes the plans that can run an L x L lattice on the
+ * current device (tiles and shared memory fit, and at least one cluster can
+ * be scheduled) into ctas[i], threads[i] for i < max_plans -- the plan
+ * rbim_sweeps_clustered uses first -- and returns how many there are (0
+ * outside the engine's range).  rbim_sweeps_clustered_plan is
+ * rbim_sweeps_clustered with an explicit plan, which must be one of
+ * rbim_cluster_plans(l_max) (RBIM_ERR_INVALID otherwise); a lattice of the
+ * call that the plan cannot run is rejected with RBIM_STATUS_BAD_CHAIN.
+ * Results do not depend on the plan: tiles start on 128-site chunk
+ * boundaries, so every plan draws the same Philox numbers.  Same reference
+ * correspondence as rbim_sweeps_clustered (src/rbim/simulation.py:196-242,
+ * many tasks at once).
+ */
+int rbim_cluster_plans(int64_t L, int *ctas, int *threads, int max_plans);
+int rbim_sweeps_clustered_plan(rbim_chain_t *chains, int n_chains, int64_t l_max, int cluster_ctas, int threads,
+                               uint32_t *spin_pool, const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64,
+                               int32_t *records, int n_sweeps, int32_t *status, void *workspace,
+                               size_t workspace_bytes, void *stream);
+
+/*
  * Plain sweeps of one chain (device descriptor `chain`) through the
  * global-memory engine: one lattice per launch sequence, any L >= 3, the
  * drop-in for one run_single_realization task.  L must equal chain->L.  Same

@@ -25,6 +25,7 @@ __all__ = [
     "plane_words",
     "resident_max_l",
     "cluster_max_l",
+    "cluster_plans",
     "engine_buckets",
     "EXPORTED_SYMBOLS",
 ]
@@ -72,6 +73,8 @@ EXPORTED_SYMBOLS = (
     "rbim_cluster_size",
     "rbim_cluster_threads",
     "rbim_sweeps_clustered",
+    "rbim_cluster_plans",
+    "rbim_sweeps_clustered_plan",
     "rbim_noalloc_max_l",
     "rbim_sweeps_plain_noalloc",
 )
@@ -123,6 +126,10 @@ def _declare(l):
     l.rbim_cluster_threads.argtypes = [c_i64]
     l.rbim_sweeps_clustered.restype = c_int
     l.rbim_sweeps_clustered.argtypes = [p, c_int, c_i64, p, p, p, p, p, c_int, p, p, c_size, p]
+    l.rbim_cluster_plans.restype = c_int
+    l.rbim_cluster_plans.argtypes = [c_i64, p, p, c_int]
+    l.rbim_sweeps_clustered_plan.restype = c_int
+    l.rbim_sweeps_clustered_plan.argtypes = [p, c_int, c_i64, c_int, c_int, p, p, p, p, p, c_int, p, p, c_size, p]
     l.rbim_noalloc_max_l.restype = c_int
     l.rbim_noalloc_max_l.argtypes = []
     l.rbim_sweeps_plain_noalloc.restype = c_int
@@ -189,6 +196,21 @@ def engine_buckets(Ls, r_max: int, c_max: int):
         else:
             key_of[L] = (2, 0)
     return [key_of[int(L)] for L in Ls]
+
+
+def cluster_plans(L: int):
+    """Cluster-engine plans ``(CTAs per cluster, CTA size)`` that can run an L x L lattice on the current device,
+    the default plan first (``rbim_cluster_plans``)."""
+    import ctypes
+
+    l = lib()
+    n = int(l.rbim_cluster_plans(int(L), None, None, 0))
+    if n <= 0:
+        return []
+    c = (ctypes.c_int * n)()
+    t = (ctypes.c_int * n)()
+    l.rbim_cluster_plans(int(L), c, t, n)
+    return [(int(c[i]), int(t[i])) for i in range(n)]
 
 
 def cluster_max_l() -> int:

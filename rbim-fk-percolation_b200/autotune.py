@@ -1,16 +1,23 @@
-"""Launch-shape autotuner for the resident engine.
+"""Launch-shape autotuner for the on-chip engines.
 
-The resident engine runs one lattice per CTA; the CTA size (threads per
-lattice, hence sites per thread) is a free parameter whose best value depends
-on the lattice size and on the device.  ``rbim_sweeps_batched`` picks it by a
-fixed rule when called with ``threads = 0``; this module times the candidates
-instead, on a synthetic batch of lattices of the launch's largest L, once per
-(device, L), and keeps the winner.  Results do not depend on the CTA size (canonical
-labels, sums in sweep order), so tuning changes speed only.
+* Resident engine (one lattice per CTA): the CTA size -- threads per lattice,
+  hence sites per thread -- is a free parameter whose best value depends on
+  the lattice size and on the device.  ``rbim_sweeps_batched`` picks it by a
+  fixed rule when called with ``threads = 0``.
+* Cluster engine (one lattice per thread-block cluster): the plan -- CTAs per
+  cluster and CTA size, hence the tile shape, the number of tile boundaries
+  the merge stage handles, and the CTAs per SM -- is picked by a fixed rule
+  in ``rbim_sweeps_clustered``; ``rbim_cluster_plans`` lists the others the
+  device can run.
+
+This module times the candidates instead, on a synthetic batch of lattices of
+the launch's largest L, once per (device, L), and keeps the winner.  Results
+do not depend on either choice (canonical labels, sums in sweep order, the
+same Philox numbers on every tile split), so tuning changes speed only.
 
 Use ``enable()`` (or set ``RBIM_AUTOTUNE=1``) to make ``ChainSet.run_batched``
-consult the tuner for every resident launch; ``RBIM_TUNE_CACHE`` names a JSON
-file that keeps the choices across processes.
+and the scan server consult the tuner for every on-chip launch;
+``RBIM_TUNE_CACHE`` names a JSON file that keeps the choices across processes.
 """
 
 from __future__ import annotations
@@ -22,13 +29,16 @@ from typing import Dict, Optional, Sequence
 
 import numpy as np
 
-__all__ = ["CANDIDATES", "size_class", "enabled", "enable", "disable", "tuned_threads", "tune", "cache"]
+__all__ = ["CANDIDATES", "size_class", "enabled", "enable", "disable", "tuned_threads", "tune", "cache",
+           "tune_cluster", "tuned_cluster_plan"]
 
 #: CTA sizes the resident engine accepts.
 CANDIDATES = (64, 128, 256, 512, 1024)
 
 _lock = threading.Lock()
-_cache: Dict[str, int] = {}
+# "<device>|<L>" -> CTA size; "<device>|cluster|<L>" -> [CTAs per cluster, CTA size]
+_cache: Dict[str, object] = {}
+_plans: Dict[str, list] = {}  # "<device>|<L>" -> the plans rbim_cluster_plans lists
 _enabled = os.environ.get("RBIM_AUTOTUNE", "") not in ("", "0")
 _loaded = False
 
@@ -40,6 +50,17 @@ def size_class(L: int) -> int:
 
 def _key(device_name: str, L: int) -> str:
     return f"{device_name}|{L}"
+
+
+def _cluster_key(device_name: str, L: int) -> str:
+    return f"{device_name}|cluster|{L}"
+
+
+def _valid(key: str, v) -> bool:
+    if "|cluster|" in key:
+        return isinstance(v, (list, tuple)) and len(v) == 2 and all(isinstance(x, int) for x in v) and \
+            v[1] in (512, 1024) and 2 <= v[0] <= 16
+    return isinstance(v, int) and v in CANDIDATES
 
 
 def _cache_path() -> Optional[str]:
@@ -56,7 +77,7 @@ def _load() -> None:
         try:
             with open(path) as f:
                 data = json.load(f)
-            _cache.update({str(k): int(v) for k, v in data.items() if int(v) in CANDIDATES})
+            _cache.update({str(k): v for k, v in data.items() if _valid(str(k), v)})
         except (OSError, ValueError, TypeError):
             pass
 
@@ -71,8 +92,9 @@ def _save() -> None:
     os.replace(tmp, path)
 
 
-def cache() -> Dict[str, int]:
-    """A copy of the tuned choices, keyed ``"<device name>|<L>"``."""
+def cache() -> Dict[str, object]:
+    """A copy of the tuned choices: ``"<device name>|<L>"`` -> CTA size of the resident engine,
+    ``"<device name>|cluster|<L>"`` -> ``[CTAs per cluster, CTA size]`` of the cluster engine."""
     with _lock:
         _load()
         return dict(_cache)
@@ -159,3 +181,98 @@ def tuned_threads(L: int, device) -> int:
         if key in _cache:
             return _cache[key]
     return tune(L, device)
+
+
+# ---------------------------------------------------------------------------
+# Cluster engine plans.
+# ---------------------------------------------------------------------------
+def plans(L: int, device) -> list:
+    """The plans ``(CTAs per cluster, CTA size)`` that can run an L x L lattice on ``device``, default first."""
+    import torch
+
+    from . import engine
+
+    rb = engine._package()
+    dev = engine.require_cuda(device)
+    key = _key(torch.cuda.get_device_name(dev), int(L))
+    with _lock:
+        if key in _plans:
+            return list(_plans[key])
+    with torch.cuda.device(dev):
+        found = rb._native.cluster_plans(int(L))
+    with _lock:
+        _plans[key] = found
+    return list(found)
+
+
+def _time_plan(rb, L: int, plan, device, n_chains: int, sweeps: int) -> float:
+    import torch
+
+    rng = np.random.default_rng(L)
+    n_real = max(1, n_chains // 4)
+    couplings = [rb.packing.pack_couplings(np.where(rng.random(2 * L * L) < 0.05, -1, 1).astype(np.int8), L)
+                 for _ in range(n_real)]
+    temps = np.linspace(1.4, 2.6, 4)
+    specs = [rb.ChainSpec(L=L, realization=k % n_real, key=104729 * (k + 1), beta=1.0 / temps[k % 4], n_therm=0,
+                          n_bins=1, sweeps_per_bin=10 * sweeps + 10) for k in range(n_chains)]
+    cs = rb.ChainSet(specs, couplings, device=device)
+    cs.init_spins(hot=True)
+    cs._run_batched_fixed(1, 0, cluster_plan=plan)
+    torch.cuda.synchronize(cs.device)
+    best = float("inf")
+    for _ in range(2):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cs._run_batched_fixed(sweeps, 0, cluster_plan=plan)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    cs.check_status()
+    return best
+
+
+def tune_cluster(L: int, device=None, sweeps: int = 2, n_chains: Optional[int] = None, candidates=None):
+    """Time every plan of ``plans(L)`` (or ``candidates``) on a synthetic batch of L x L lattices; return and
+    remember the fastest ``(CTAs per cluster, CTA size)``."""
+    import torch
+
+    from . import engine
+
+    rb = engine._package()
+    dev = engine.require_cuda(device)
+    name = torch.cuda.get_device_name(dev)
+    cands = [tuple(c) for c in (candidates or plans(L, dev))]
+    if not cands:
+        raise ValueError(f"no cluster plan can run L = {L} on this device")
+    if n_chains is None:
+        # Two full waves of the plan with the fewest CTAs per cluster.
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        n_chains = max(8, 2 * sms // min(c for c, _ in cands))
+    times = {c: _time_plan(rb, int(L), c, dev, n_chains, sweeps) for c in cands}
+    best = min(times, key=times.get)
+    with _lock:
+        _load()
+        _cache[_cluster_key(name, int(L))] = [int(best[0]), int(best[1])]
+        _save()
+    return (int(best[0]), int(best[1]))
+
+
+def tuned_cluster_plan(l_max: int, sizes: Sequence[int], device):
+    """The tuned plan of a cluster launch of lattices ``sizes`` (largest ``l_max``), tuning it on first use; None
+    when tuning is off, or when the tuned plan cannot run every size of the launch (the default plan then runs)."""
+    if not _enabled:
+        return None
+    import torch
+
+    name = torch.cuda.get_device_name(device)
+    key = _cluster_key(name, int(l_max))
+    with _lock:
+        _load()
+        plan = _cache.get(key)
+    if plan is None:
+        plan = tune_cluster(int(l_max), device)
+    plan = (int(plan[0]), int(plan[1]))
+    if all(plan in [tuple(p) for p in plans(L, device)] for L in sizes):
+        return plan
+    return None

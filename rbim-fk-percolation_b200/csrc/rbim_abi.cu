@@ -1,5 +1,6 @@
 // C ABI of librbim_sm100 (declared in include/rbim_sm100.h): argument checks,
 // error reporting and dispatch to the resident and plain engines.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <mutex>
@@ -282,6 +283,60 @@ int rbim_sweeps_clustered(rbim_chain_t *chains, int n_chains, int64_t l_max, uin
                                                 (long long *)acc_int, acc_f64, records, n_sweeps, (int *)workspace,
                                                 status, (cudaStream_t)stream);
     return cuda_check(e, "rbim_sweeps_clustered");
+}
+
+int rbim_cluster_plans(int64_t L, int *ctas, int *threads, int max_plans)
+{
+    if (L <= rbim::resident_max_l() || L > 65535 || max_plans < 0) return 0;
+    const uint32_t l = (uint32_t)L;
+    const rbim::ClusterPlan def = rbim::cluster_plan(l);
+    int n = 0;
+    auto consider = [&](rbim::ClusterPlan p) {
+        if (!rbim::cluster_plan_ok(l, p)) return;
+        int clusters = 0;
+        if (rbim::cluster_occupancy_plan(l, p, &clusters) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (clusters <= 0) return;
+        if (n < max_plans && ctas && threads) {
+            ctas[n] = (int)p.C;
+            threads[n] = (int)p.threads;
+        }
+        ++n;
+    };
+    if (def.C) consider(def);
+    for (uint32_t t : {1024u, 512u})
+        for (uint32_t C = 2; C <= 16u; ++C)
+            if (!(C == def.C && t == def.threads)) consider({C, t});
+    return n;
+}
+
+int rbim_sweeps_clustered_plan(rbim_chain_t *chains, int n_chains, int64_t l_max, int cluster_ctas, int threads,
+                               uint32_t *spin_pool, const uint32_t *coupling_pool, int64_t *acc_int, double *acc_f64,
+                               int32_t *records, int n_sweeps, int32_t *status, void *workspace,
+                               size_t workspace_bytes, void *stream)
+{
+    if (n_chains < 0 || n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_chains and n_sweeps must be >= 0");
+    if (n_chains == 0 || n_sweeps == 0) return RBIM_OK;
+    if (int rc = check_chain_sizes(l_max)) return rc;
+    if (l_max <= rbim::resident_max_l())
+        return fail(RBIM_ERR_INVALID, "l_max = %lld is small enough for rbim_sweeps_batched (limit %d)",
+                    (long long)l_max, rbim::resident_max_l());
+    if (l_max > 65535) return fail(RBIM_ERR_UNSUPPORTED, "l_max = %lld is beyond the cluster engine", (long long)l_max);
+    const rbim::ClusterPlan plan{(uint32_t)std::max(cluster_ctas, 0), (uint32_t)std::max(threads, 0)};
+    if (!rbim::cluster_plan_ok((uint32_t)l_max, plan))
+        return fail(RBIM_ERR_INVALID, "plan of %d CTAs of %d threads cannot run L = %lld (see rbim_cluster_plans)",
+                    cluster_ctas, threads, (long long)l_max);
+    if (!chains || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status || !workspace)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    if (!aligned16(spin_pool) || !aligned16(coupling_pool))
+        return fail(RBIM_ERR_INVALID, "spin and coupling pools must be 16-byte aligned");
+    if (workspace_bytes < rbim_batched_workspace_bytes()) return fail(RBIM_ERR_INVALID, "workspace too small");
+    cudaError_t e = rbim::launch_cluster_sweeps_plan(chains, n_chains, (int)l_max, plan, spin_pool, coupling_pool,
+                                                     (long long *)acc_int, acc_f64, records, n_sweeps,
+                                                     (int *)workspace, status, (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_clustered_plan");
 }
 
 size_t rbim_plain_workspace_bytes(int64_t L) { return L < 3 ? 0 : rbim::plain_workspace_bytes(L); }

@@ -137,6 +137,13 @@ ClusterPlan cluster_plan(uint32_t L)
 
 uint32_t cluster_size_for(uint32_t L) { return cluster_plan(L).C; }
 
+bool cluster_plan_ok(uint32_t L, ClusterPlan p)
+{
+    if (p.C < 2u || p.C > kClusterMax || (p.threads != 512u && p.threads != 1024u)) return false;
+    const uint32_t cap = p.threads == 512u ? kTileHalf : kTileMax;
+    return cluster_tiles_ok(L, p.C, cap) && cluster_layout_fits(cluster_layout(L, p.C), p.threads);
+}
+
 namespace {
 
 // Shared scratch of one CTA of the cluster.
@@ -1026,16 +1033,16 @@ struct Launch {
     ClusterLayout ly;
 };
 
-Launch launch_for(uint32_t l_max)
+// The launch of a plan: the classes with a compile-time layout (4 CTAs of
+// 1024 threads up to L = 512, 16 up to L = 1024) take it whatever L they run,
+// any other plan the run-time layout of l_max.
+Launch launch_for(uint32_t l_max, ClusterPlan plan)
 {
-    const ClusterPlan plan = cluster_plan(l_max);
     Launch l{plan.threads, 0u, plan.C, {}};
     if (plan.C == 0) return l;
-    const ClusterPlan p512 = cluster_plan(512u), p1024 = cluster_plan(1024u);
-    if (plan.threads == p512.threads && plan.C == p512.C && l_max <= 512u && p512.threads == 1024u && p512.C == 4u)
+    if (plan.threads == 1024u && plan.C == 4u && l_max <= 512u && cluster_plan_ok(512u, plan))
         l.lc = 512u;
-    else if (plan.threads == p1024.threads && plan.C == p1024.C && l_max <= 1024u && p1024.threads == 1024u &&
-             p1024.C == 16u)
+    else if (plan.threads == 1024u && plan.C == 16u && l_max <= 1024u && cluster_plan_ok(1024u, plan))
         l.lc = 1024u;
     l.ly = cluster_layout(l.lc ? l.lc : l_max, plan.C);
     return l;
@@ -1043,10 +1050,12 @@ Launch launch_for(uint32_t l_max)
 
 }  // namespace
 
-cudaError_t cluster_occupancy(uint32_t l_max, int *clusters)
+cudaError_t cluster_occupancy(uint32_t l_max, int *clusters) { return cluster_occupancy_plan(l_max, cluster_plan(l_max), clusters); }
+
+cudaError_t cluster_occupancy_plan(uint32_t l_max, ClusterPlan plan, int *clusters)
 {
     *clusters = 0;
-    const Launch l = launch_for(l_max);
+    const Launch l = launch_for(l_max, plan);
     if (l.C == 0 || !cluster_layout_fits(l.ly, l.threads)) return cudaSuccess;
     if (l.lc == 512) return occupancy_t<1024, 512, 4>(l.ly, l.C, clusters);
     if (l.lc == 1024) return occupancy_t<1024, 1024, 16>(l.ly, l.C, clusters);
@@ -1058,7 +1067,16 @@ cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int 
                                   const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
                                   int n_sweeps, int *queue, int *status, cudaStream_t stream)
 {
-    const Launch l = launch_for((uint32_t)l_max);
+    return launch_cluster_sweeps_plan(chains, n_chains, l_max, cluster_plan((uint32_t)l_max), spin_pool,
+                                      coupling_pool, acc_i, acc_f, rec, n_sweeps, queue, status, stream);
+}
+
+cudaError_t launch_cluster_sweeps_plan(const rbim_chain_t *chains, int n_chains, int l_max, ClusterPlan plan,
+                                       uint32_t *spin_pool, const uint32_t *coupling_pool, long long *acc_i,
+                                       double *acc_f, int32_t *rec, int n_sweeps, int *queue, int *status,
+                                       cudaStream_t stream)
+{
+    const Launch l = launch_for((uint32_t)l_max, plan);
     if (l.C == 0) return cudaErrorInvalidValue;
     if (!cluster_layout_fits(l.ly, l.threads)) return cudaErrorInvalidConfiguration;
     if (l.lc == 512)

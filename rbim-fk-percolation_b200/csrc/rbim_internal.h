@@ -70,12 +70,19 @@ struct ClusterPlan {
     uint32_t C, threads;
 };
 ClusterPlan cluster_plan(uint32_t L);
+// A plan the engine can run an L x L lattice with (tiles fit, layout fits).
+bool cluster_plan_ok(uint32_t L, ClusterPlan p);
 uint32_t cluster_size_for(uint32_t L);
 ClusterLayout cluster_layout(uint32_t l_max, uint32_t C);
 bool cluster_layout_fits(const ClusterLayout &ly, uint32_t threads);
 cudaError_t cluster_occupancy(uint32_t l_max, int *clusters);
+cudaError_t cluster_occupancy_plan(uint32_t l_max, ClusterPlan plan, int *clusters);
 cudaError_t launch_cluster_sweeps(const rbim_chain_t *chains, int n_chains, int l_max, uint32_t *spin_pool,
                                   const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *rec,
                                   int n_sweeps, int *queue, int *status, cudaStream_t stream);
+cudaError_t launch_cluster_sweeps_plan(const rbim_chain_t *chains, int n_chains, int l_max, ClusterPlan plan,
+                                       uint32_t *spin_pool, const uint32_t *coupling_pool, long long *acc_i,
+                                       double *acc_f, int32_t *rec, int n_sweeps, int *queue, int *status,
+                                       cudaStream_t stream);
 
 }  // namespace rbim

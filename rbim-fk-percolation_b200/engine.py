@@ -69,13 +69,16 @@ def _side(device, n: int):
 @dataclass
 class Launch:
     """One on-chip launch of a call: ``kind`` 0 resident (``rbim_sweeps_batched``) or 1 cluster
-    (``rbim_sweeps_clustered``), over ``count`` consecutive descriptors at device address ``chains``."""
+    (``rbim_sweeps_clustered``), over ``count`` consecutive descriptors at device address ``chains``.
+    A cluster launch with ``ctas > 0`` runs the plan (``ctas`` CTAs of ``threads``) through
+    ``rbim_sweeps_clustered_plan``."""
 
     kind: int
     chains: int
     count: int
     l_max: int
     threads: int = 0
+    ctas: int = 0
 
 
 def launch_buckets(lib, device, stream, launches: Sequence[Launch], *, spin_pool: int, coupling_pool: int,
@@ -112,6 +115,11 @@ def launch_buckets(lib, device, stream, launches: Sequence[Launch], *, spin_pool
             rc = lib.rbim_sweeps_batched(p(b.chains), b.count, b.l_max, p(spin_pool), p(coupling_pool), p(acc_int),
                                          p(acc_f64), rec, int(n_sweeps), int(b.threads), p(status), ws, QUEUE_SLOT, sp)
             _native.check(rc, "rbim_sweeps_batched")
+        elif b.kind == 1 and b.ctas > 0:
+            rc = lib.rbim_sweeps_clustered_plan(p(b.chains), b.count, b.l_max, int(b.ctas), int(b.threads),
+                                                p(spin_pool), p(coupling_pool), p(acc_int), p(acc_f64), rec,
+                                                int(n_sweeps), p(status), ws, QUEUE_SLOT, sp)
+            _native.check(rc, "rbim_sweeps_clustered_plan")
         elif b.kind == 1:
             rc = lib.rbim_sweeps_clustered(p(b.chains), b.count, b.l_max, p(spin_pool), p(coupling_pool), p(acc_int),
                                            p(acc_f64), rec, int(n_sweeps), p(status), ws, QUEUE_SLOT, sp)
@@ -254,12 +262,14 @@ class ChainSet:
         self.slot = np.empty(self.n, dtype=np.int64)
         self.slot[order] = np.arange(self.n)
         self.buckets = []  # (kind, first slot, count, l_max)
+        self.bucket_sizes = []  # the distinct L of each bucket
         groups = {}
         for i, k in enumerate(keys):
             groups.setdefault(k, []).append(i)
         for k in sorted(groups):
             members = np.array(groups[k], dtype=np.int64)
             self.buckets.append((k[0], int(self.slot[members].min()), len(members), int(Ls[members].max())))
+            self.bucket_sizes.append(sorted(set(int(v) for v in Ls[members])))
         self.plain_only = [int(i) for i in order if keys[i][0] == 2]
 
         desc = np.zeros(self.n, dtype=_native.CHAIN_DTYPE)
@@ -349,22 +359,28 @@ class ChainSet:
         """
         self._run_batched_fixed(n_sweeps, threads, tuned=threads == 0, concurrent=concurrent)
 
-    def _run_batched_fixed(self, n_sweeps: int, threads: int, tuned: bool = False, concurrent: bool = True) -> None:
+    def _run_batched_fixed(self, n_sweeps: int, threads: int, tuned: bool = False, concurrent: bool = True,
+                           cluster_plan=None) -> None:
+        """``cluster_plan`` ``(CTAs, CTA size)`` fixes the plan of every cluster launch (the tuner's timing runs)."""
         if n_sweeps <= 0:
             return
         from . import autotune
         torch = _torch()
         launches = []
-        for kind, first, count, l_max in self.buckets:
+        for (kind, first, count, l_max), sizes in zip(self.buckets, self.bucket_sizes):
             if kind == 2:
                 continue
-            nt = 0
+            ctas = 0
             if kind == 0:
                 nt = autotune.tuned_threads(l_max, self.device) if tuned else threads
                 nt = nt or int(self.lib.rbim_resident_threads(l_max))
             else:
-                nt = int(self.lib.rbim_cluster_threads(l_max))
-            launches.append(Launch(kind, self.chains.data_ptr() + 96 * first, count, l_max, nt))
+                plan = cluster_plan or (autotune.tuned_cluster_plan(l_max, sizes, self.device) if tuned else None)
+                if plan:
+                    ctas, nt = int(plan[0]), int(plan[1])
+                else:
+                    nt = int(self.lib.rbim_cluster_threads(l_max))
+            launches.append(Launch(kind, self.chains.data_ptr() + 96 * first, count, l_max, nt, ctas))
         if launches:
             ws = self._workspace(QUEUE_SLOT * len(launches))
             with torch.cuda.device(self.device):

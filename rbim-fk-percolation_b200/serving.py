@@ -384,7 +384,11 @@ class ScanServer:
                     nt = nt or int(self.lib.rbim_resident_threads(l_max))
                     on_chip.append(Launch(0, base, count, l_max, nt))
                 elif key[0] == 1:
-                    on_chip.append(Launch(1, base, count, l_max, int(self.lib.rbim_cluster_threads(l_max))))
+                    plan = autotune.tuned_cluster_plan(l_max, sorted({a.plan.L for a in group}), self.device)
+                    if plan:
+                        on_chip.append(Launch(1, base, count, l_max, plan[1], plan[0]))
+                    else:
+                        on_chip.append(Launch(1, base, count, l_max, int(self.lib.rbim_cluster_threads(l_max))))
                 else:
                     plain += [(int(allc["L"][first + k]), base + 96 * k) for k in range(count)]
                 first += count

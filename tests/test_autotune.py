@@ -68,3 +68,66 @@ def test_tune_picks_a_candidate_and_run_batched_uses_it(rb, monkeypatch, tmp_pat
     for name, entry in plain["observables"].items():
         for field, v in entry.items():
             np.testing.assert_array_equal(tuned["observables"][name][field], v)
+
+
+def test_cluster_plan_cache_entries(rb, tmp_path, monkeypatch):
+    at = rb.autotune
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"GPU X|cluster|512": [4, 1024], "GPU X|cluster|300": [3, 333],
+                                "GPU X|cluster|724": [1, 1024], "GPU X|64": 128}))
+    monkeypatch.setenv("RBIM_TUNE_CACHE", str(path))
+    monkeypatch.setattr(at, "_loaded", False)
+    monkeypatch.setattr(at, "_cache", {})
+    assert at.cache() == {"GPU X|cluster|512": [4, 1024], "GPU X|64": 128}
+    monkeypatch.setattr(at, "_enabled", False)
+    assert at.tuned_cluster_plan(512, [512], None) is None
+
+
+def test_cluster_plans_host_query(rb):
+    """The plan list is empty outside the cluster engine's range, and the CTA counts are cluster sizes."""
+    lib = rb._native.lib()
+    assert lib.rbim_cluster_plans(rb._native.resident_max_l(), None, None, 0) == 0
+    assert lib.rbim_cluster_plans(70000, None, None, 0) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L", [300, 512])
+def test_results_do_not_depend_on_cluster_plan(rb, L):
+    """Every plan rbim_cluster_plans lists gives the default plan's spins, bin sums and records bit for bit (tile
+    boundaries fall elsewhere, the Philox numbers do not)."""
+    plans = rb._native.cluster_plans(L)
+    assert plans and plans[0] == (rb._native.lib().rbim_cluster_size(L), rb._native.lib().rbim_cluster_threads(L))
+    rng = np.random.default_rng(L)
+    J = [rb.packing.pack_couplings(np.where(rng.random(2 * L * L) < 0.1, -1, 1).astype(np.int8), L) for _ in range(2)]
+    specs = [rb.ChainSpec(L=L, realization=k % 2, key=31 * k + 7, beta=1.0 / (1.6 + 0.3 * k), n_therm=1, n_bins=2,
+                          sweeps_per_bin=2, records=True) for k in range(3)]
+    out = []
+    for plan in plans:
+        cs = rb.ChainSet(specs, J)
+        cs.init_spins(hot=True)
+        cs._run_batched_fixed(5, 0, cluster_plan=plan)
+        cs.check_status()
+        ai, af = cs.all_bins()
+        out.append((plan, ai, af.view(np.int64), cs.spin_pool.cpu().numpy(), cs.records.cpu().numpy()))
+    for o in out[1:]:
+        for a, b in zip(out[0][1:], o[1:]):
+            assert np.array_equal(a, b), o[0]
+
+
+@pytest.mark.gpu
+def test_tune_cluster_picks_a_listed_plan(rb, monkeypatch, tmp_path):
+    at = rb.autotune
+    monkeypatch.setenv("RBIM_TUNE_CACHE", str(tmp_path / "t.json"))
+    monkeypatch.setattr(at, "_loaded", False)
+    monkeypatch.setattr(at, "_cache", {})
+    L = 320
+    best = at.tune_cluster(L, n_chains=12, sweeps=1)
+    assert best in rb._native.cluster_plans(L)
+    monkeypatch.setattr(at, "_enabled", True)
+    kw = dict(L=L, p=0.08, temperatures=[1.6, 2.4], n_realizations=2, n_sweeps=6, n_therm=2, n_bins=2, seed=5)
+    tuned = rb.run_temperature_scan(**kw, engine="batched")
+    monkeypatch.setattr(at, "_enabled", False)
+    default = rb.run_temperature_scan(**kw, engine="batched")
+    for name, entry in default["observables"].items():
+        for field, v in entry.items():
+            np.testing.assert_array_equal(tuned["observables"][name][field], v)
