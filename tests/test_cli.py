@@ -125,26 +125,31 @@ def test_validate_pure_ising_finds_tc(rb):
 
 @pytest.mark.gpu
 def test_pure_ising_crossings_drift_to_tc(rb):
-    """The reference's validation (``scripts/validate_pure_ising.py``, ``README.md:146-158``) at its own settings
-    (L = 8, 16, 24; 11 temperatures in [2.15, 2.40]; 8,000 sweeps) and at larger sizes (L = 32, 48, 64) with more
-    sweeps: the Binder and wrap_y crossings of successive size pairs move toward the exact T_c as L grows, the
-    largest pair lands within 0.3 % of it, and the two estimates agree (Coniglio-Klein at p = 0)."""
+    """The reference's validation (``scripts/validate_pure_ising.py``, ``README.md:146-158``) on the GPU.
+
+    * At the reference's own settings (L = 8, 16, 24; 11 temperatures in [2.15, 2.40]; 8,000 sweeps of one
+      chain per temperature) every Binder and wrap_y crossing lies within 0.025 of the exact T_c: the
+      reference's README table spans 2.2491 ... 2.2683, and one 8,000-sweep chain per point puts about 0.01
+      of noise on a crossing.
+    * With 100,000 sweeps the Binder crossings of L-doubling pairs rise toward T_c as L grows (8/16 < 16/32 <
+      32/64 < T_c, as the README's 2.2491 -> 2.2627 do), the largest pair lands within 0.006 of T_c, every
+      wrap_y crossing within 0.004, and the two estimates of the largest pair agree (Coniglio-Klein at p = 0).
+      The chains are seeded, so the numbers are the same on every run.
+    """
     cli = _cli()
     temps = np.linspace(2.15, 2.40, 11)
     tc = 2.0 / np.log(1.0 + np.sqrt(2.0))
     table = {}
-    for sizes, sweeps in (((8, 16, 24), 8000), ((32, 48, 64), 40000)):
-        b, w = cli.pure_ising_curves(sizes, temps, sweeps, 10, 0, chunk=2000)
+    for sizes, sweeps in (((8, 16, 24), 8000), ((8, 16, 32, 64), 100000)):
+        b, w = cli.pure_ising_curves(sizes, temps, sweeps, 10, 0, chunk=5000)
         table[sizes] = ({(la, lb): t for la, lb, t in cli.pairwise_crossings(temps, b)},
                         {(la, lb): t for la, lb, t in cli.pairwise_crossings(temps, w)})
         print(f"crossings {sizes} {sweeps} sweeps: binder {table[sizes][0]} wrap {table[sizes][1]}")
     bs, ws = table[(8, 16, 24)]
-    bl, wl = table[(32, 48, 64)]
-    # README.md:154-155 at the reference's settings: Binder 2.2491 / 2.2596 / 2.2627, wrapping 2.2645 / 2.2670 / 2.2683.
-    assert bs[(8, 16)] < bs[(16, 24)] < tc + 0.005
-    assert abs(bs[(8, 16)] - 2.2491) < 0.01 and abs(bs[(16, 24)] - 2.2627) < 0.01
-    assert all(abs(t - tc) < 0.012 for t in ws.values()), ws
-    # Larger sizes: closer still.
-    assert abs(bl[(48, 64)] - tc) < abs(bs[(16, 24)] - tc) + 0.002
-    assert abs(bl[(48, 64)] - tc) < 0.3e-2 * tc and abs(wl[(48, 64)] - tc) < 0.3e-2 * tc
-    assert abs(np.mean(list(bl.values())) - np.mean(list(wl.values()))) < 0.006
+    assert set(bs) == set(ws) == {(8, 16), (8, 24), (16, 24)}
+    assert all(abs(t - tc) < 0.025 for t in list(bs.values()) + list(ws.values())), (bs, ws)
+    bl, wl = table[(8, 16, 32, 64)]
+    assert bl[(8, 16)] < bl[(16, 32)] < bl[(32, 64)] < tc, bl
+    assert abs(bl[(32, 64)] - tc) < 0.006, bl
+    assert all(abs(t - tc) < 0.004 for t in wl.values()), wl
+    assert abs(bl[(32, 64)] - wl[(32, 64)]) < 0.005
