@@ -719,7 +719,9 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 }
             }
             __syncthreads();
-            phase_sites<Word16>(t, warp, nwarps, true, false);
+            // Flip run pieces by their tile root's FLIP bit; a measured sweep
+            // also leaves every piece leader's word holding its tile root.
+            flip_pieces(t, tid, NT, measure);
             __syncthreads();
             cl.sync();  // every flip is done
             tile_halo<NT>(x, tl, cl, red, tid);
@@ -744,29 +746,30 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
             // piece may hold all 65536 sites).
             count_pieces<true>(t, u16, warp, nwarps);
             __syncthreads();
-            // OV (no longer needed this sweep) becomes the plane of node marks.
-            for (uint32_t w = tid; w < t.g.NW; w += NT) t.OV[w] = 0u;
+            // FLIP (no longer needed this sweep) becomes the plane of node
+            // marks; OV still gives the run pieces of the |M_C| pass.
+            for (uint32_t w = tid; w < t.g.NW; w += NT) t.FLIP[w] = 0u;
             __syncthreads();
-            // Merged sizes into the root nodes; mark this tile's nodes in OV.
+            // Merged sizes into the root nodes; mark this tile's nodes in FLIP.
             uint32_t rootnodes = 0;
             for (uint32_t k = tid; k < x.hs; k += NT) {
                 const uint32_t m = x.HK[k];
                 if (m == kEmptyKey) continue;
                 const uint32_t r = node_root(x, k);
-                atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
+                atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
                 unsigned int *hi = (unsigned int *)(cl.map_shared_rank(x.HW, r >> 16) + (r & 0xFFFFu)) + 1;
                 atomicAdd(hi, (unsigned int)u16[m] + 1u);
                 if (r == ((c << 16) | k)) ++rootnodes;
             }
             __syncthreads();
             uint32_t nloc = rootnodes;
-            for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~t.OV[w]);
+            for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~t.FLIP[w]);
             cl.sync();  // merged sizes are complete
 
             // Local top two: tile-only clusters and this tile's root nodes.
             unsigned long long k1 = 0, k2 = 0;
             for (uint32_t w = tid; w < t.g.NW; w += NT) {
-                uint32_t roots = t.ROOT[w] & ~t.OV[w];
+                uint32_t roots = t.ROOT[w] & ~t.FLIP[w];
                 while (roots) {
                     const uint32_t bb = __ffs(roots) - 1u;
                     roots &= roots - 1u;
@@ -863,11 +866,11 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
             const bool second = records && ch.rec_off >= 0;
             if (many) {
                 // Tile roots of the largest cluster, marked in OH, and with
-                // `second` those of the second largest in OV (whose node
+                // `second` those of the second largest in FLIP (whose node
                 // marks are no longer needed).
                 for (uint32_t w = tid; w < t.g.NW; w += NT) {
                     t.OH[w] = 0u;
-                    if (second) t.OV[w] = 0u;
+                    if (second) t.FLIP[w] = 0u;
                 }
                 __syncthreads();
                 if (tid == 0 && g1 >= tl.b && g1 < tl.b + tl.Tc) {
@@ -876,7 +879,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 }
                 if (second && tid == 0 && g2 >= tl.b && g2 < tl.b + tl.Tc) {
                     const uint32_t m = g2 - tl.b;
-                    atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
+                    atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
                 }
                 for (uint32_t k = tid; k < x.hs; k += NT) {
                     if (x.HK[k] == kEmptyKey) continue;
@@ -888,26 +891,33 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                         atomicOr(t.OH + (m >> 5), 1u << (m & 31u));
                     } else if (second && gr == g2) {
                         const uint32_t m = x.HK[k];
-                        atomicOr(t.OV + (m >> 5), 1u << (m & 31u));
+                        atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
                     }
                 }
                 __syncthreads();
                 int mc = 0, mc2 = 0;
-                for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
-                    const uint32_t n = (w << 5) + lane;
-                    bool in = false, in2 = false;
-                    if (n < t.g.N) {
-                        const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
-                        in = (t.OH[r >> 5] >> (r & 31u)) & 1u;
-                        if (second) in2 = (t.OV[r >> 5] >> (r & 31u)) & 1u;
+                // One lane per word, one test per run piece: a piece leader's
+                // word holds its tile root (the root's own word its size).
+                for (uint32_t w = tid; w < t.g.NW; w += NT) {
+                    const uint32_t valid = t.g.valid(w);
+                    uint32_t lead = piece_leaders(t, w, valid);
+                    const uint32_t roots = t.ROOT[w], sw = t.S[w];
+                    const uint32_t nv = (uint32_t)__popc(valid);
+                    while (lead) {
+                        const uint32_t b = __ffs(lead) - 1u;
+                        lead &= lead - 1u;
+                        const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
+                        const uint32_t n = (w << 5) + b;
+                        const uint32_t r = ((roots >> b) & 1u) ? n : (uint32_t)u16[n];
+                        const uint32_t pm = (end - b == 32u) ? 0xFFFFFFFFu : (((1u << (end - b)) - 1u) << b);
+                        const int m = (int)__popc(pm) - 2 * (int)__popc(pm & sw);
+                        if ((t.OH[r >> 5] >> (r & 31u)) & 1u) mc += m;
+                        if (second && ((t.FLIP[r >> 5] >> (r & 31u)) & 1u)) mc2 += m;
                     }
-                    const uint32_t sw = t.S[w];
-                    const uint32_t mm = __ballot_sync(0xFFFFFFFFu, in);
-                    if (lane == 0) mc += (int)__popc(mm) - 2 * (int)__popc(mm & sw);
-                    if (second) {
-                        const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, in2);
-                        if (lane == 0) mc2 += (int)__popc(m2) - 2 * (int)__popc(m2 & sw);
-                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    mc += __shfl_xor_sync(0xFFFFFFFFu, mc, o);
+                    mc2 += __shfl_xor_sync(0xFFFFFFFFu, mc2, o);
                 }
                 if (lane == 0) {
                     red.mcw[warp] = mc;

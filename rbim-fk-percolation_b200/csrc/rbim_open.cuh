@@ -323,4 +323,43 @@ __device__ __forceinline__ void count_pieces(const Lat<Word16> &t, unsigned shor
     }
 }
 
+// Root of any site n once the roots pass is done: every parent is a run head
+// (heads are the initial parents, roots are heads, and hooks, path halving
+// and the seam merge only ever point at roots or grandparents) and every head
+// then points at its root (a root at itself), so two loads reach it.
+__device__ __forceinline__ uint32_t piece_root(const unsigned short *u16, uint32_t n) { return u16[u16[n]]; }
+
+// The cluster flip of a sweep, one lane per word and one root lookup per run
+// piece instead of per site: the sites of a word split into pieces (maximal
+// runs of occupied y-bonds cut at the word boundary) that share a root, and a
+// piece flips as a whole when its root's FLIP bit is set.  With
+// `leader_roots` the leader of every piece that does not head its run (bit 0
+// of a word inside a run) also gets its root written, so that afterwards the
+// word of every piece leader holds its root, which the cluster-size count and
+// the |M_C| pass read.  Non-head words are nobody's parent, so the writes do
+// not disturb the lookups of other lanes.
+__device__ __forceinline__ void flip_pieces(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads,
+                                                     bool leader_roots)
+{
+    const Geom &g = t.g;
+    unsigned short *u16 = t.uf.w;
+    for (uint32_t w = tid; w < g.NW; w += nthreads) {
+        const uint32_t valid = g.valid(w);
+        const uint32_t heads = head_mask(t.OV, w, valid);
+        uint32_t lead = (heads | 1u) & valid;
+        const uint32_t nv = (uint32_t)__popc(valid);
+        uint32_t fl = 0;
+        while (lead) {
+            const uint32_t b = __ffs(lead) - 1u;
+            lead &= lead - 1u;
+            const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
+            const uint32_t n = (w << 5) + b;
+            const uint32_t r = piece_root(u16, n);
+            if ((t.FLIP[r >> 5] >> (r & 31u)) & 1u) fl |= (end - b == 32u) ? 0xFFFFFFFFu : (((1u << (end - b)) - 1u) << b);
+            if (leader_roots && !((heads >> b) & 1u)) u16[n] = (unsigned short)r;
+        }
+        if (fl) t.S[w] ^= fl;
+    }
+}
+
 }  // namespace rbim
