@@ -52,6 +52,12 @@ struct UF<Word16> {
     {
         asm volatile("st.volatile.shared.u16 [%0], %1;" ::"r"(sa + 2u * i), "h"(v) : "memory");
     }
+    // The parents of sites i and i + 1 (i even) in one 32-bit store: v holds
+    // site i's in its low half.
+    __device__ __forceinline__ void st2(uint32_t i, uint32_t v) const
+    {
+        asm volatile("st.volatile.shared.u32 [%0], %1;" ::"r"(sa + 2u * i), "r"(v) : "memory");
+    }
     __device__ __forceinline__ T cas(uint32_t i, T expect, T v) const
     {
         T old;

@@ -242,16 +242,38 @@ __device__ __forceinline__ void phase_heads(const Lat<WT> &t, uint32_t warp, uin
         // Last head before word j: the scan of lanes < j, or pre for j = 0.
         uint32_t before = __shfl_up_sync(0xFFFFFFFFu, incl, 1);
         if (lane == 0) before = pre;
-        for (uint32_t j = 0; j < B; ++j) {
-            const uint32_t w = base + j;
-            if (w >= g.NW) break;
-            const uint32_t hj = __shfl_sync(0xFFFFFFFFu, h, j);
-            const uint32_t cj = __shfl_sync(0xFFFFFFFFu, before, j);
-            const uint32_t n = (w << 5) + lane;
-            if (n < g.N) {
-                const uint32_t m = hj & mask_le(lane);
-                const uint32_t head = m ? (w << 5) + 31u - __clz(m) : cj - 1u;
-                t.uf.st(n, WT::make(head, 0, 0));
+        if constexpr (sizeof(typename WT::T) == 2) {
+            // 16-bit parents: two words per step, each lane writing the parents
+            // of two neighbouring sites with one 32-bit store (lanes 0-15 word
+            // j, lanes 16-31 word j + 1); sites past N are not written.
+            const uint32_t half = lane >> 4, b0 = 2u * (lane & 15u);
+            for (uint32_t j = 0; j < B; j += 2u) {
+                const uint32_t jj = j + half;
+                const uint32_t hj = __shfl_sync(0xFFFFFFFFu, h, jj & 31u);
+                const uint32_t cj = __shfl_sync(0xFFFFFFFFu, before, jj & 31u);
+                const uint32_t w = base + jj;
+                if (jj >= B || w >= g.NW) continue;
+                const uint32_t n = (w << 5) + b0;
+                const uint32_t m0 = hj & mask_le(b0), m1 = hj & mask_le(b0 + 1u);
+                const uint32_t h0 = m0 ? (w << 5) + 31u - __clz(m0) : cj - 1u;
+                const uint32_t h1 = m1 ? (w << 5) + 31u - __clz(m1) : cj - 1u;
+                if (n + 1u < g.N)
+                    t.uf.st2(n, h0 | (h1 << 16));
+                else if (n < g.N)
+                    t.uf.st(n, WT::make(h0, 0, 0));
+            }
+        } else {
+            for (uint32_t j = 0; j < B; ++j) {
+                const uint32_t w = base + j;
+                if (w >= g.NW) break;
+                const uint32_t hj = __shfl_sync(0xFFFFFFFFu, h, j);
+                const uint32_t cj = __shfl_sync(0xFFFFFFFFu, before, j);
+                const uint32_t n = (w << 5) + lane;
+                if (n < g.N) {
+                    const uint32_t m = hj & mask_le(lane);
+                    const uint32_t head = m ? (w << 5) + 31u - __clz(m) : cj - 1u;
+                    t.uf.st(n, WT::make(head, 0, 0));
+                }
             }
         }
     }

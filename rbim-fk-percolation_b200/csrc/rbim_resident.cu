@@ -510,26 +510,50 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         RBIM_PHASE_MARK(8);
         const uint32_t g1 = red.g1, g2 = red.g2;
         int mc = 0, mc2 = 0;
-        // One lane per word, one test per run piece: the word of a piece's
-        // leader holds its root (its size counter when the leader is the
-        // root, recognised by its ROOT bit).  Measured faster on B200 than
-        // lanes-as-sites with the root read from each site's piece leader
-        // (15 k vs 24 k cycles per L = 256 sweep).
-        for (uint32_t w = tid; w < g.NW; w += NT) {
-            const uint32_t valid = g.valid(w);
-            uint32_t lead = piece_leaders(t, w, valid);
-            const uint32_t roots = t.ROOT[w], s = t.S[w];
-            const uint32_t nv = (uint32_t)__popc(valid);
-            while (lead) {
-                const uint32_t b = __ffs(lead) - 1u;
-                lead &= lead - 1u;
-                const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
-                const uint32_t n = (w << 5) + b;
-                const uint32_t r = ((roots >> b) & 1u) ? n : (uint32_t)u16[n];
-                const uint32_t pm = (end - b == 32u) ? 0xFFFFFFFFu : (((1u << (end - b)) - 1u) << b);
-                const int m = (int)__popc(pm) - 2 * (int)__popc(pm & s);
-                if (r == g1) mc += m;
-                if (second && r == g2) mc2 += m;
+        if (g.NW < NT) {
+            // Small lattices took the per-site path (every site's word holds
+            // its root): lanes are sites, which keeps all warps busy.  Two
+            // words per iteration keep two load chains in flight.
+            for (uint32_t w0 = warp; w0 < g.NW; w0 += 2u * nwarps) {
+                const uint32_t w1 = w0 + nwarps;
+                const uint32_t n0 = (w0 << 5) + lane, n1 = (w1 << 5) + lane;
+                const uint32_t rt0 = t.ROOT[w0], rt1 = w1 < g.NW ? t.ROOT[w1] : 0u;
+                const bool ok0 = n0 < g.N, ok1 = n1 < g.N;
+                const uint32_t p0 = ok0 ? (uint32_t)u16[n0] : 0u, p1 = ok1 ? (uint32_t)u16[n1] : 0u;
+                const uint32_t r0 = ((rt0 >> lane) & 1u) ? n0 : p0, r1 = ((rt1 >> lane) & 1u) ? n1 : p1;
+                const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, ok0 && r0 == g1);
+                const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, ok1 && r1 == g1);
+                const uint32_t s0 = t.S[w0], s1 = w1 < g.NW ? t.S[w1] : 0u;
+                if (lane == 0) mc += (int)__popc(m0) - 2 * (int)__popc(m0 & s0) + (int)__popc(m1) - 2 * (int)__popc(m1 & s1);
+                if (second) {
+                    const uint32_t q0 = __ballot_sync(0xFFFFFFFFu, ok0 && r0 == g2);
+                    const uint32_t q1 = __ballot_sync(0xFFFFFFFFu, ok1 && r1 == g2);
+                    if (lane == 0) mc2 += (int)__popc(q0) - 2 * (int)__popc(q0 & s0) + (int)__popc(q1) -
+                                          2 * (int)__popc(q1 & s1);
+                }
+            }
+        } else {
+            // One lane per word, one test per run piece: the word of a piece's
+            // leader holds its root (its size counter when the leader is the
+            // root, recognised by its ROOT bit).  Measured faster on B200 than
+            // lanes-as-sites with the root read from each site's piece leader
+            // (15 k vs 24 k cycles per L = 256 sweep).
+            for (uint32_t w = tid; w < g.NW; w += NT) {
+                const uint32_t valid = g.valid(w);
+                uint32_t lead = piece_leaders(t, w, valid);
+                const uint32_t roots = t.ROOT[w], s = t.S[w];
+                const uint32_t nv = (uint32_t)__popc(valid);
+                while (lead) {
+                    const uint32_t b = __ffs(lead) - 1u;
+                    lead &= lead - 1u;
+                    const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
+                    const uint32_t n = (w << 5) + b;
+                    const uint32_t r = ((roots >> b) & 1u) ? n : (uint32_t)u16[n];
+                    const uint32_t pm = (end - b == 32u) ? 0xFFFFFFFFu : (((1u << (end - b)) - 1u) << b);
+                    const int m = (int)__popc(pm) - 2 * (int)__popc(pm & s);
+                    if (r == g1) mc += m;
+                    if (second && r == g2) mc2 += m;
+                }
             }
         }
 #pragma unroll
