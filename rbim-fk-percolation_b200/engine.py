@@ -26,8 +26,11 @@ __all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_M
            "launch_buckets"]
 
 #: A set of one lattice runs on the plain engine under ``engine="auto"`` when
-#: its L exceeds this (measured on B200: below it one resident CTA is faster).
-PLAIN_SINGLE_MIN_L = 128
+#: its L exceeds this.  Measured on B200 with the plain engine's launch
+#: sequence replayed as a CUDA graph: one resident CTA is faster at L = 48
+#: (20.8 k against 18.5 k sweeps/s), the plain engine from L = 64 up (20.1 k
+#: against 18.9 k at L = 64, 18.9 k against 16.0 k at L = 128).
+PLAIN_SINGLE_MIN_L = 56
 
 
 def auto_engine(specs) -> str:
@@ -292,6 +295,8 @@ class ChainSet:
         self.n_total = np.array([s.n_total for s in self.specs], dtype=np.int64)
         self._sweep_host = np.zeros(self.n, dtype=np.int64)
         self._ws = None
+        self._pws = None  # plain-engine workspace; captured graphs hold its address
+        self._graphs = {}  # (sweeps, chain indices) -> torch.cuda.CUDAGraph of run_plain
 
     # -- helpers -----------------------------------------------------------
     @staticmethod
@@ -398,22 +403,74 @@ class ChainSet:
         else:
             self._sweep_host = np.minimum(self._sweep_host + n_sweeps, self.n_total)
 
-    def run_plain(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> None:
-        """Advance chains one at a time on the plain (global-memory) engine."""
+    #: ``run_plain`` replays a captured CUDA graph for calls of at least this
+    #: many sweeps: the plain engine issues 7 kernels per sweep, which at small
+    #: L cost more to launch one by one than to run.
+    PLAIN_GRAPH_MIN_SWEEPS = 8
+    #: ... and of at most this many kernel nodes (7 per sweep per chain).
+    PLAIN_GRAPH_MAX_NODES = 1 << 15
+
+    def _plain_workspace(self, idx):
+        nbytes = max(int(self.lib.rbim_plain_workspace_bytes(self.specs[i].L)) for i in idx)
+        if self._pws is None or self._pws.numel() < nbytes:
+            self._graphs.clear()  # they hold the old workspace's address
+            self._pws = _torch().empty(max(nbytes, 256), dtype=_torch().uint8, device=self.device)
+        return self._pws
+
+    def _launch_plain(self, n_sweeps: int, idx, ws, stream) -> None:
+        for i in idx:
+            rc = self.lib.rbim_sweeps_plain(
+                self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * int(self.slot[i])), self._ptr(self.spin_pool),
+                self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
+                self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
+                self._ptr(self.status), self._ptr(ws), ws.numel(), stream)
+            _native.check(rc, "rbim_sweeps_plain")
+
+    def _plain_graph_ok(self, n_sweeps: int, idx) -> bool:
+        return n_sweeps >= self.PLAIN_GRAPH_MIN_SWEEPS and 7 * n_sweeps * len(idx) <= self.PLAIN_GRAPH_MAX_NODES
+
+    def capture_plain(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> bool:
+        """Capture the launch sequence of ``run_plain(n_sweeps, chains)`` as a CUDA graph without running it.
+
+        Every kernel reads the chain descriptors from device memory (a finished
+        chain's kernels return at once), so one graph serves every later call
+        with the same arguments.  Returns False when the call is outside the
+        graph limits and ``run_plain`` would launch directly.
+        """
+        idx = list(range(self.n)) if chains is None else [int(i) for i in chains]
+        if n_sweeps <= 0 or not self._plain_graph_ok(n_sweeps, idx):
+            return False
+        key = (int(n_sweeps), tuple(idx))
+        ws = self._plain_workspace(idx)
+        if key not in self._graphs:
+            torch = _torch()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.device(self.device):
+                s = torch.cuda.Stream(self.device)
+                with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+                    self._launch_plain(n_sweeps, idx, ws, ctypes.c_void_p(s.cuda_stream))
+            self._graphs[key] = g
+        return True
+
+    def run_plain(self, n_sweeps: int, chains: Optional[Sequence[int]] = None, graph: bool = True) -> None:
+        """Advance chains one at a time on the plain (global-memory) engine.
+
+        With ``graph`` (the default), calls of at least
+        ``PLAIN_GRAPH_MIN_SWEEPS`` sweeps replay a CUDA graph of the launch
+        sequence, captured on the first such call (``capture_plain``); the
+        results are the same as launching one by one.
+        """
         if n_sweeps <= 0:
             return
-        idx = range(self.n) if chains is None else chains
-        nbytes = max(int(self.lib.rbim_plain_workspace_bytes(self.specs[i].L)) for i in idx)
-        ws = self._workspace(nbytes)
-        with _torch().cuda.device(self.device):
-            for i in idx:
-                rc = self.lib.rbim_sweeps_plain(
-                    self.specs[i].L, ctypes.c_void_p(self.chains.data_ptr() + 96 * int(self.slot[i])), self._ptr(self.spin_pool),
-                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
-                    self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
-                    self._ptr(self.status), self._ptr(ws), ws.numel(), self._stream())
-                _native.check(rc, "rbim_sweeps_plain")
-                self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
+        idx = list(range(self.n)) if chains is None else [int(i) for i in chains]
+        torch = _torch()
+        with torch.cuda.device(self.device):
+            if graph and self.capture_plain(n_sweeps, idx):
+                self._graphs[(int(n_sweeps), tuple(idx))].replay()
+            else:
+                self._launch_plain(n_sweeps, idx, self._plain_workspace(idx), self._stream())
+        for i in idx:
+            self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
 
     def run_plain_noalloc(self, n_sweeps: int, chains: Optional[Sequence[int]] = None) -> None:
         """As :meth:`run_plain`, through ``rbim_sweeps_plain_noalloc`` (library-static scratch, L <= 512).
@@ -441,11 +498,12 @@ class ChainSet:
     def run_to_end(self, engine: str = "auto", chunk: int = 1000, threads: int = 0) -> None:
         """Run every chain to the end of its run in chunks of ``chunk`` sweeps.
 
-        ``engine="auto"`` runs a set of one lattice with L > 128 on the plain
-        engine, whose whole grid works on the one lattice (on B200 a sweep of
-        one L = 256 lattice takes 78 us there against 169 us on one resident
-        CTA, L = 1024 172 us against 211 us on one 16-CTA cluster), and any
-        other set on the batched engines.  Results are the same either way.
+        ``engine="auto"`` runs a set of one lattice with L > PLAIN_SINGLE_MIN_L
+        on the plain engine, whose whole grid works on the one lattice (on
+        B200 a sweep of one L = 256 lattice takes 60 us there against 160 us
+        on one resident CTA, L = 1024 150 us against 200 us on one 16-CTA
+        cluster), and any other set on the batched engines.  Results are the
+        same either way.
         """
         if engine == "auto":
             engine = auto_engine(self.specs)

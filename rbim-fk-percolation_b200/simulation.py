@@ -245,7 +245,7 @@ def run_single_realization(L: int, J: np.ndarray, temperature: float, *, n_sweep
 
     ``engine``: ``"plain"`` (global-memory engine, one lattice per launch
     sequence), ``"batched"`` (resident or cluster engine, one CTA or one
-    cluster for the lattice) or ``"auto"`` (plain for L > 128, where the whole
+    cluster for the lattice) or ``"auto"`` (plain for L > 56, where the whole
     grid on one lattice beats one CTA or one cluster; batched otherwise).
     Every engine gives the same result.
     """

@@ -212,3 +212,24 @@ def test_single_realization_engines_agree(rb, L):
         for k, v in out["auto"].bin_primitives.items():
             assert np.array_equal(np.asarray(v, np.float64).view(np.uint64),
                                   np.asarray(out[e].bin_primitives[k], np.float64).view(np.uint64)), (e, k)
+
+
+@pytest.mark.parametrize("L", [24, 200])
+def test_plain_graph_replay_equals_direct_launches(rb, L):
+    """run_plain replays a captured CUDA graph of its launch sequence; the state after any mix of replayed and
+    directly launched calls equals the state after direct launches alone, bit for bit."""
+    out = []
+    for graph in (True, False):
+        J = _couplings(L, 0.1, 5)
+        spec = rb.ChainSpec(L=L, realization=0, key=42, beta=1 / 2.1, n_therm=3, n_bins=3, sweeps_per_bin=9,
+                            records=True)
+        cs = rb.ChainSet([spec], [rb.packing.pack_couplings(J, L)])
+        cs.init_spins(hot=True)
+        for n in (8, 8, 3, 8, 100):
+            cs.run_plain(n, graph=graph)
+        cs.check_status()
+        assert (len(cs._graphs) == 2) == graph  # calls of 8 and of 100 sweeps
+        out.append((cs.acc_int.cpu().numpy(), cs.acc_f64.cpu().numpy().view(np.int64), cs.spin_pool.cpu().numpy(),
+                    cs.records.cpu().numpy(), cs.device_sweeps()))
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
