@@ -331,8 +331,13 @@ class ChainSet:
         No check is made beyond the field's type: this is how a caller sets
         ``walk_cap`` or, in tests, a descriptor the kernels must reject.
         """
+        self.set_descriptor_fields(i, **{name: value})
+
+    def set_descriptor_fields(self, i: int, **fields) -> None:
+        """Write several fields of chain ``i``'s ``rbim_chain_t`` with one copy to the device."""
         k = int(self.slot[i])
-        self.desc_host[name][k] = value
+        for name, value in fields.items():
+            self.desc_host[name][k] = value
         row = _torch().from_numpy(self.desc_host[k: k + 1].view(np.uint8).copy())
         self.chains[96 * k: 96 * (k + 1)].copy_(row)
 

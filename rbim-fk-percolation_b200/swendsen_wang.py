@@ -8,14 +8,15 @@ which keep the state on the device across sweeps.
 
 from __future__ import annotations
 
+import threading
 from dataclasses import dataclass
 from typing import Optional
 
 import numpy as np
 
-from .engine import ChainSet, ChainSpec
+from .engine import ChainSet, ChainSpec, _torch, require_cuda
 from .lattice import Lattice
-from .packing import pack_couplings, pack_spins
+from .packing import pack_couplings, pack_spins, threshold, words_for
 
 __all__ = [
     "SweepResult",
@@ -83,27 +84,53 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
     """One Swendsen-Wang update of ``spins`` in place (reference ``swendsen_wang.py:103-172``).
 
     Randomness comes from the Philox stream of ``key`` at sweep counter
-    ``sweep``; when ``key`` is omitted it is drawn from ``rng``.
+    ``sweep``; when ``key`` is omitted it is drawn from ``rng``.  The device
+    buffers of L x L lattices are kept between calls (one chain set per device
+    and L, used under a lock), so a loop over ``sw_sweep`` allocates device
+    memory only on its first call; each call still copies the spins and
+    couplings in and the spins and the record out.
     """
     L = lattice.L
     if key is None:
         if rng is None:
             raise ValueError("sw_sweep needs a key or a numpy Generator")
         key = int(rng.integers(0, 2**63, dtype=np.int64))
-    # One chain whose only sweep is `sweep`: measured when n_therm == sweep.
-    spec = ChainSpec(L=L, realization=0, key=int(key) & (2**64 - 1), beta=beta,
-                     n_therm=sweep if measure else sweep + 1, n_bins=1, sweeps_per_bin=1, records=measure)
-    cs = ChainSet([spec], [pack_couplings(J, L)], device=device)
-    cs.set_sweep(0, sweep)
-    cs.set_spins(0, pack_spins(spins, L))
-    cs.run_plain(1)
-    cs.check_status()
-    spins[...] = cs.spins(0).astype(spins.dtype)
-    if not measure:
-        return None
-    rec = cs.chain_records(0)[0]
+    cs, lock = _sweep_chain_set(L, device)
+    with lock:
+        # One chain whose only sweep is `sweep`: measured when n_therm == sweep.
+        cs.coupling_pool[: 2 * words_for(L)].copy_(_torch().from_numpy(pack_couplings(J, L).view(np.int32)))
+        cs.set_spins(0, pack_spins(spins, L))
+        cs.set_descriptor_fields(0, key=int(key) & (2**64 - 1), thr=threshold(beta), sweep=sweep,
+                                 n_therm=sweep if measure else sweep + 1, n_bins=1, sweeps_per_bin=1)
+        cs.acc_int.zero_()
+        cs.acc_f64.zero_()
+        cs.run_plain(1)
+        cs.check_status()
+        spins[...] = cs.spins(0).astype(spins.dtype)
+        if not measure:
+            return None
+        rec = cs.chain_records(0)[0]
     wx = bool(rec[7]) if measure_percolation else None
     wy = bool(rec[8]) if measure_percolation else None
     return SweepResult(energy=float(rec[0]), magnetization=float(rec[1]), n_clusters=int(rec[2]),
                        largest_size=int(rec[3]), largest_abs_magnetization=float(rec[4]), second_size=int(rec[5]),
                        second_abs_magnetization=float(rec[6]), wraps_x=wx, wraps_y=wy)
+
+
+_sets_lock = threading.Lock()
+_sets = {}  # (device, L) -> (ChainSet of one chain with a one-row record buffer, its lock)
+
+
+def _sweep_chain_set(L: int, device):
+    """The device state ``sw_sweep`` reuses for L x L lattices: one chain set per (device, L), created on first
+    use, so that a caller looping over ``sw_sweep`` does not allocate and free device buffers every sweep."""
+    dev = require_cuda(device)
+    key = (str(dev), int(L))
+    with _sets_lock:
+        entry = _sets.get(key)
+        if entry is None:
+            spec = ChainSpec(L=L, realization=0, key=0, beta=1.0, n_therm=0, n_bins=1, sweeps_per_bin=1, records=True)
+            cs = ChainSet([spec], [np.zeros(2 * words_for(L), dtype="<u4")], device=dev)
+            entry = (cs, threading.Lock())
+            _sets[key] = entry
+        return entry

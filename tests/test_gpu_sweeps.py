@@ -199,7 +199,7 @@ def test_sw_sweep_api_matches_oracle(rb, orc):
         assert np.array_equal(spins, ref.astype(np.int64))
 
 
-@pytest.mark.parametrize("L", [100, 160])
+@pytest.mark.parametrize("L", [48, 100, 160])
 def test_single_realization_engines_agree(rb, L):
     """run_single_realization gives the same sums on every engine; engine="auto" takes the plain engine for one
     lattice with L > PLAIN_SINGLE_MIN_L and the resident engine below."""
