@@ -173,7 +173,7 @@ struct Red {
     uint32_t unsat[NT / 32], downs[NT / 32], roots[NT / 32];
     int mc[NT / 32], mc2[NT / 32];
     int item, wrap, err;
-    uint32_t ncl, g1, g2, s1, s2, unsat_t, downs_t;
+    uint32_t g1, g2, s1, s2;
     // State of the chain being processed; only thread 0 updates it.
     Acc acc;
     long long cur_bin;
@@ -436,17 +436,9 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
     const Geom &g = t.g;
     unsigned short *u16 = t.uf.w;
 
-    // Energy and magnetization of the flipped spins; root counters to zero.
+    // Energy and magnetization of the flipped spins.
     uint32_t unsat = 0, downs = 0;
     measure_energy(t, tid, NT, unsat, downs);
-    for (uint32_t w = tid; w < g.NW; w += NT) {
-        uint32_t roots = t.ROOT[w];
-        while (roots) {
-            const uint32_t b = __ffs(roots) - 1u;
-            roots &= roots - 1u;
-            u16[(w << 5) + b] = 0;
-        }
-    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         unsat += __shfl_xor_sync(0xFFFFFFFFu, unsat, o);
@@ -457,28 +449,23 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         red.downs[warp] = downs;
         red.roots[warp] = nroots_warp;
     }
-    __syncthreads();
     RBIM_PHASE_MARK(6);
-    if (warp == 0) {
-        uint32_t u = lane < nwarps ? red.unsat[lane] : 0u, d = lane < nwarps ? red.downs[lane] : 0u;
-        uint32_t nr = lane < nwarps ? red.roots[lane] : 0u;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            u += __shfl_xor_sync(0xFFFFFFFFu, u, o);
-            d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
-            nr += __shfl_xor_sync(0xFFFFFFFFu, nr, o);
-        }
-        if (lane == 0) {
-            red.ncl = nr;
-            red.unsat_t = u;
-            red.downs_t = d;
-        }
-    }
-    // Cluster sizes into the root words.
+    // Cluster sizes into the root words, on top of the index each root's word
+    // holds (a root points at itself): afterwards a root's word is root + size
+    // mod 2^16, which gives every size whenever there are two or more
+    // clusters (each then below 65536); one cluster is the lattice.
     count_pieces<false>(t, u16, warp, nwarps);
     __syncthreads();
     RBIM_PHASE_MARK(7);
-    const uint32_t ncl = red.ncl;
+    // Every warp sums the per-warp partials itself (no barrier needed after).
+    uint32_t unsat_t = lane < nwarps ? red.unsat[lane] : 0u, downs_t = lane < nwarps ? red.downs[lane] : 0u;
+    uint32_t ncl = lane < nwarps ? red.roots[lane] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsat_t += __shfl_xor_sync(0xFFFFFFFFu, unsat_t, o);
+        downs_t += __shfl_xor_sync(0xFFFFFFFFu, downs_t, o);
+        ncl += __shfl_xor_sync(0xFFFFFFFFu, ncl, o);
+    }
     if (ncl > 1) {
         uint32_t k1 = 0, k2 = 0;
         for (uint32_t w = tid; w < g.NW; w += NT) {
@@ -487,7 +474,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
                 const uint32_t b = __ffs(roots) - 1u;
                 roots &= roots - 1u;
                 const uint32_t r = (w << 5) + b;
-                top2_merge(k1, k2, ((uint32_t)u16[r] << 16) | (0xFFFFu - r), 0u);
+                top2_merge(k1, k2, ((((uint32_t)u16[r] - r) & 0xFFFFu) << 16) | (0xFFFFu - r), 0u);
             }
         }
         warp_top2(k1, k2);
@@ -573,7 +560,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
         red.s1 = g.N;
         red.s2 = 0;
     }
-    const long long M = (long long)g.N - 2ll * (long long)red.downs_t;
+    const long long M = (long long)g.N - 2ll * (long long)downs_t;
     if (tid == 0) {
         long long mc_total = M, mc2_total = 0;
         if (ncl > 1) {
@@ -583,7 +570,7 @@ __device__ __forceinline__ void resident_measure(const Res &res, Red<NT> &red, u
                 mc2_total += red.mc2[i];
             }
         }
-        rec[0] = 2ll * (long long)red.unsat_t - 2ll * (long long)g.N;
+        rec[0] = 2ll * (long long)unsat_t - 2ll * (long long)g.N;
         rec[1] = M;
         rec[2] = ncl;
         rec[3] = red.s1;
