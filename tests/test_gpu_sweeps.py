@@ -233,3 +233,26 @@ def test_plain_graph_replay_equals_direct_launches(rb, L):
                     cs.records.cpu().numpy(), cs.device_sweeps()))
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_sw_sweep_reused_state_does_not_leak(rb, orc):
+    """sw_sweep keeps one device chain set per L; calls that alternate sizes, couplings, keys, temperatures and
+    measured or unmeasured sweeps each still equal the oracle's sweep."""
+    cases = []
+    for L, seed in ((12, 1), (20, 2), (12, 3), (20, 4), (12, 1)):
+        J = _couplings(L, 0.15, seed)
+        spins = orc.initial_spins(L * L, 100 + seed, hot=True).astype(np.int64)
+        cases.append((L, J, spins, 100 + seed))
+    for step in range(3):
+        for L, J, spins, key in cases:
+            T = 1.6 + 0.3 * step
+            measure = step != 1
+            ref = spins.astype(np.int8).copy()
+            res = rb.sw_sweep(spins, rb.build_lattice(L), J, 1 / T, key=key, sweep=step, measure=measure)
+            r = orc.sw_sweep(L, ref, J, key, rb.packing.threshold(1 / T), step, measure=measure)
+            assert np.array_equal(spins, ref.astype(np.int64)), (L, key, step)
+            if measure:
+                assert (res.energy, res.magnetization, res.n_clusters, res.largest_size, res.second_size,
+                        res.second_abs_magnetization) == (r[0], r[1], r[2], r[3], r[5], r[6])
+            else:
+                assert res is None
