@@ -60,9 +60,11 @@ enum {
 enum {
     RBIM_STATUS_FIND_CAP = 1,  /* a union-find walk exceeded its bound */
     RBIM_STATUS_UNION_CAP = 2, /* a union retried beyond its bound */
-    RBIM_STATUS_BAD_CHAIN = 4  /* a chain descriptor was out of range: L outside the call's range (or, on the
+    RBIM_STATUS_BAD_CHAIN = 4, /* a chain descriptor was out of range: L outside the call's range (or, on the
                                   plain path, different from the call's L), sweeps_per_bin < 1, n_bins < 0,
                                   n_therm < 0 or walk_cap < 0; the chain is skipped and left unchanged */
+    RBIM_STATUS_GRID_WAIT = 8  /* grid engine: a CTA waited at a grid-wide barrier beyond its bound; every CTA
+                                  then stops waiting and runs to its end, and the chain's state is undefined */
 };
 
 /*
@@ -234,6 +236,38 @@ size_t rbim_plain_workspace_bytes(int64_t L);
 int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool, int64_t *acc_int,
                       double *acc_f64, int32_t *records, int n_sweeps, int32_t *status, void *workspace,
                       size_t workspace_bytes, void *stream);
+
+/*
+ * Grid sweeps of one chain (device descriptor `chain`): one lattice over the
+ * whole GPU in a single cooperative launch per call, the drop-in for one
+ * run_single_realization task (src/rbim/simulation.py:196-242) for
+ * 32 < L <= about 3000.  The launch's C CTAs each keep one tile of at most
+ * 65536 consecutive sites in shared memory for every sweep of the call; the
+ * clusters that cross tile boundaries or the periodic seams are merged in a
+ * union-find in global memory between grid-wide barriers.  L must equal
+ * chain->L.  Same accumulator and record contract (and the same results, bit
+ * for bit) as rbim_sweeps_plain.
+ *
+ * A plan is (ctas, threads): ctas tiles, threads per CTA (256, 512 or 1024).
+ * rbim_grid_plan writes the default plan for the current device (one
+ * 1024-thread CTA per SM, fewer CTAs when tiles would hold fewer than L
+ * sites) and returns RBIM_OK, or RBIM_ERR_UNSUPPORTED when no plan fits L.
+ * rbim_grid_workspace_bytes(L, ctas) is the workspace a plan of `ctas` CTAs
+ * needs (ctas = 0: the default plan's); it holds one 8-byte union-find word
+ * per site.  rbim_sweeps_grid takes ctas = threads = 0 for the default plan.
+ * The whole grid must be resident at once: a plan with more CTAs than the
+ * device holds returns RBIM_ERR_CUDA (cudaErrorCooperativeLaunchTooLarge).
+ *
+ * Every wait at a grid-wide barrier gives up after wait_cycles SM clock
+ * cycles (0: about one second) and sets RBIM_STATUS_GRID_WAIT; the launch
+ * then runs to its end without waiting again and the chain's state is
+ * undefined.  Calls sharing a workspace must be ordered (one stream).
+ */
+int rbim_grid_plan(int64_t L, int *ctas, int *threads);
+size_t rbim_grid_workspace_bytes(int64_t L, int ctas);
+int rbim_sweeps_grid(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                     int64_t *acc_int, double *acc_f64, int32_t *records, int n_sweeps, int32_t *status, int ctas,
+                     int threads, int64_t wait_cycles, void *workspace, size_t workspace_bytes, void *stream);
 
 /*
  * rbim_sweeps_plain without a caller workspace.  No counterpart in the

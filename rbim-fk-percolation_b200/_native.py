@@ -77,6 +77,9 @@ EXPORTED_SYMBOLS = (
     "rbim_sweeps_clustered_plan",
     "rbim_noalloc_max_l",
     "rbim_sweeps_plain_noalloc",
+    "rbim_grid_plan",
+    "rbim_grid_workspace_bytes",
+    "rbim_sweeps_grid",
 )
 
 
@@ -134,6 +137,12 @@ def _declare(l):
     l.rbim_noalloc_max_l.argtypes = []
     l.rbim_sweeps_plain_noalloc.restype = c_int
     l.rbim_sweeps_plain_noalloc.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, p]
+    l.rbim_grid_plan.restype = c_int
+    l.rbim_grid_plan.argtypes = [c_i64, p, p]
+    l.rbim_grid_workspace_bytes.restype = c_size
+    l.rbim_grid_workspace_bytes.argtypes = [c_i64, c_int]
+    l.rbim_sweeps_grid.restype = c_int
+    l.rbim_sweeps_grid.argtypes = [c_i64, p, p, p, p, p, p, c_int, p, c_int, c_int, c_i64, p, c_size, p]
 
 
 def lib(build_if_missing: bool = True):
@@ -211,6 +220,17 @@ def cluster_plans(L: int):
     t = (ctypes.c_int * n)()
     l.rbim_cluster_plans(int(L), c, t, n)
     return [(int(c[i]), int(t[i])) for i in range(n)]
+
+
+def grid_plan(L: int):
+    """Default grid-engine plan ``(CTAs, CTA size)`` for one L x L lattice on the current device, or None
+    (``rbim_grid_plan``)."""
+    import ctypes
+
+    c, t = ctypes.c_int(0), ctypes.c_int(0)
+    if lib().rbim_grid_plan(int(L), ctypes.byref(c), ctypes.byref(t)) != 0:
+        return None
+    return int(c.value), int(t.value)
 
 
 def cluster_max_l() -> int:

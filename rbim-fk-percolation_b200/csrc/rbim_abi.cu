@@ -358,6 +358,53 @@ int rbim_sweeps_plain(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const
     return cuda_check(e, "rbim_sweeps_plain");
 }
 
+int rbim_grid_plan(int64_t L, int *ctas, int *threads)
+{
+    if (!ctas || !threads) return fail(RBIM_ERR_INVALID, "null pointer");
+    *ctas = 0;
+    *threads = 0;
+    if (L <= 32 || L > 65535) return fail(RBIM_ERR_UNSUPPORTED, "grid engine: L = %lld outside 33..65535", (long long)L);
+    const rbim::GridPlan p = rbim::grid_plan((uint32_t)L);
+    if (!p.C) return fail(RBIM_ERR_UNSUPPORTED, "grid engine: no plan fits L = %lld", (long long)L);
+    *ctas = (int)p.C;
+    *threads = (int)p.threads;
+    return RBIM_OK;
+}
+
+size_t rbim_grid_workspace_bytes(int64_t L, int ctas)
+{
+    if (L <= 32 || L > 65535 || ctas < 0) return 0;
+    uint32_t C = (uint32_t)ctas;
+    if (!C) C = rbim::grid_plan((uint32_t)L).C;
+    if (!C) return 0;
+    return rbim::grid_workspace_bytes((uint32_t)L, C);
+}
+
+int rbim_sweeps_grid(int64_t L, rbim_chain_t *chain, uint32_t *spin_pool, const uint32_t *coupling_pool,
+                     int64_t *acc_int, double *acc_f64, int32_t *records, int n_sweeps, int32_t *status, int ctas,
+                     int threads, int64_t wait_cycles, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (L <= 32 || L > 65535) return fail(RBIM_ERR_UNSUPPORTED, "grid engine: L = %lld outside 33..65535", (long long)L);
+    if (n_sweeps < 0) return fail(RBIM_ERR_INVALID, "n_sweeps must be >= 0");
+    if (ctas < 0 || threads < 0 || wait_cycles < 0) return fail(RBIM_ERR_INVALID, "negative plan or wait bound");
+    if (n_sweeps == 0) return RBIM_OK;
+    if (!chain || !spin_pool || !coupling_pool || !acc_int || !acc_f64 || !status || !workspace)
+        return fail(RBIM_ERR_INVALID, "null pointer");
+    rbim::GridPlan plan{(uint32_t)ctas, (uint32_t)threads};
+    if (!ctas && !threads) plan = rbim::grid_plan((uint32_t)L);
+    if (!plan.C) return fail(RBIM_ERR_UNSUPPORTED, "grid engine: no plan fits L = %lld", (long long)L);
+    if (!rbim::grid_plan_ok((uint32_t)L, plan))
+        return fail(RBIM_ERR_INVALID, "grid engine: plan (%d CTAs, %d threads) cannot run L = %lld", ctas, threads,
+                    (long long)L);
+    const size_t need = rbim::grid_workspace_bytes((uint32_t)L, plan.C);
+    if (workspace_bytes < need) return fail(RBIM_ERR_INVALID, "workspace too small: %zu < %zu", workspace_bytes, need);
+    if (((uintptr_t)workspace & 255u) != 0) return fail(RBIM_ERR_INVALID, "workspace must be 256-byte aligned");
+    cudaError_t e = rbim::launch_grid_sweeps(chain, L, plan, spin_pool, coupling_pool, (long long *)acc_int, acc_f64,
+                                             records, n_sweeps, status, workspace, (long long)wait_cycles,
+                                             (cudaStream_t)stream);
+    return cuda_check(e, "rbim_sweeps_grid");
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

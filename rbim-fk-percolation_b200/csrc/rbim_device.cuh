@@ -65,6 +65,7 @@ constexpr uint32_t kStreamBondLow = 3u;
 constexpr int kErrFindCap = 1;
 constexpr int kErrUnionCap = 2;
 constexpr int kErrBadChain = 4;
+constexpr int kErrGridWait = 8;
 
 struct U4 {
     uint32_t x, y, z, w;

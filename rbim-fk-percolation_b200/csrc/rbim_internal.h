@@ -85,4 +85,17 @@ cudaError_t launch_cluster_sweeps_plan(const rbim_chain_t *chains, int n_chains,
                                        double *acc_f, int32_t *rec, int n_sweeps, int *queue, int *status,
                                        cudaStream_t stream);
 
+
+// Grid engine (one lattice over a cooperative grid of C CTAs, one tile of at
+// most 65536 consecutive sites per CTA, tiles merged through global memory).
+struct GridPlan {
+    uint32_t C, threads;
+};
+GridPlan grid_plan(uint32_t L);
+bool grid_plan_ok(uint32_t L, GridPlan p);
+size_t grid_workspace_bytes(uint32_t L, uint32_t C);
+cudaError_t launch_grid_sweeps(rbim_chain_t *chain, int64_t L, GridPlan plan, uint32_t *spin_pool,
+                               const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *records,
+                               int n_sweeps, int *status, void *workspace, long long wait_cycles, cudaStream_t stream);
+
 }  // namespace rbim

@@ -296,6 +296,7 @@ class ChainSet:
         self._sweep_host = np.zeros(self.n, dtype=np.int64)
         self._ws = None
         self._pws = None  # plain-engine workspace; captured graphs hold its address
+        self._gws = None  # grid-engine workspace
         self._graphs = {}  # (sweeps, chain indices) -> torch.cuda.CUDAGraph of run_plain
 
     # -- helpers -----------------------------------------------------------
@@ -496,6 +497,38 @@ class ChainSet:
                 _native.check(rc, "rbim_sweeps_plain_noalloc")
                 self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
 
+    def _grid_workspace(self, L: int, ctas: int):
+        nbytes = int(self.lib.rbim_grid_workspace_bytes(int(L), int(ctas)))
+        if nbytes <= 0:
+            raise _native.RbimError(f"the grid engine has no plan for L = {L}")
+        if self._gws is None or self._gws.numel() < nbytes:
+            self._gws = _torch().empty(max(nbytes, 256), dtype=_torch().uint8, device=self.device)
+        return self._gws
+
+    def run_grid(self, n_sweeps: int, chains: Optional[Sequence[int]] = None, plan=None,
+                 wait_cycles: int = 0) -> None:
+        """Advance chains one at a time on the grid engine: one cooperative launch per chain and call, the
+        lattice split in tiles over every SM (``rbim_sweeps_grid``).
+
+        ``plan`` is ``(CTAs, CTA size)``, by default the device's (``_native.grid_plan``); results do not
+        depend on it.  ``wait_cycles`` bounds each wait at a grid-wide barrier (0: about one second).
+        """
+        if n_sweeps <= 0:
+            return
+        idx = list(range(self.n)) if chains is None else [int(i) for i in chains]
+        ctas, threads = (0, 0) if plan is None else (int(plan[0]), int(plan[1]))
+        with _torch().cuda.device(self.device):
+            for i in idx:
+                L = self.specs[i].L
+                ws = self._grid_workspace(L, ctas)
+                rc = self.lib.rbim_sweeps_grid(
+                    L, ctypes.c_void_p(self.chains.data_ptr() + 96 * int(self.slot[i])), self._ptr(self.spin_pool),
+                    self._ptr(self.coupling_pool), self._ptr(self.acc_int), self._ptr(self.acc_f64),
+                    self._ptr(self.records) if self.records is not None else None, int(n_sweeps),
+                    self._ptr(self.status), ctas, threads, int(wait_cycles), self._ptr(ws), ws.numel(), self._stream())
+                _native.check(rc, "rbim_sweeps_grid")
+                self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
+
     def remaining(self) -> int:
         """Sweeps still to run for the longest chain (host bookkeeping)."""
         return int(np.max(self.n_total - self._sweep_host))
@@ -512,12 +545,14 @@ class ChainSet:
         """
         if engine == "auto":
             engine = auto_engine(self.specs)
-        if engine not in ("batched", "plain"):
-            raise ValueError(f"engine must be 'auto', 'batched' or 'plain', got {engine!r}")
+        if engine not in ("batched", "plain", "grid"):
+            raise ValueError(f"engine must be 'auto', 'batched', 'plain' or 'grid', got {engine!r}")
         while self.remaining() > 0:
             n = min(chunk, self.remaining())
             if engine == "batched":
                 self.run_batched(n, threads)
+            elif engine == "grid":
+                self.run_grid(n)
             else:
                 self.run_plain(n)
         self.check_status()

@@ -85,7 +85,19 @@ def test_argument_errors_are_reported_without_device_work(rb):
     assert rc == -1
     rc = lib.rbim_activate(8, dummy, dummy, 1, 2**32 + 1, 0, dummy, dummy, 1 << 20, None)
     assert rc == -1 and b"thr" in lib.rbim_last_error()
+    # Grid engine: sizes, plans and workspace are checked on the host.
+    rc = lib.rbim_sweeps_grid(32, dummy, dummy, dummy, dummy, dummy, None, 5, dummy, 0, 0, 0, dummy, 1 << 30, None)
+    assert rc == -3 and b"33..65535" in lib.rbim_last_error()
+    rc = lib.rbim_sweeps_grid(64, None, None, None, None, None, None, 5, None, 0, 0, 0, None, 0, None)
+    assert rc == -1 and b"null pointer" in lib.rbim_last_error()
+    rc = lib.rbim_sweeps_grid(64, dummy, dummy, dummy, dummy, dummy, None, 5, dummy, 1000, 1024, 0, dummy, 1 << 30, None)
+    assert rc == -1 and b"cannot run" in lib.rbim_last_error()
+    rc = lib.rbim_sweeps_grid(1024, dummy, dummy, dummy, dummy, dummy, None, 5, dummy, 128, 1024, 0, dummy, 4096, None)
+    assert rc == -1 and b"workspace too small" in lib.rbim_last_error()
+    assert lib.rbim_grid_workspace_bytes(1024, 128) >= 8 * 1024 * 1024
+    assert lib.rbim_grid_workspace_bytes(32, 4) == 0
     # Zero-work calls succeed without touching the device.
+    assert lib.rbim_sweeps_grid(64, None, None, None, None, None, None, 0, None, 0, 0, 0, None, 0, None) == 0
     assert lib.rbim_sweeps_batched(None, 0, 32, None, None, None, None, None, 10, 0, None, None, 0, None) == 0
     assert lib.rbim_label_wrap(8, 0, None, None, None, None, None, None, 0, None) == 0
 
