@@ -23,11 +23,13 @@
 //  4. after a second barrier every node finds its root and takes the root's
 //     raw flip bit (published before the first barrier); the tile flips by
 //     run pieces and writes its spins back; a third barrier;
-//  5. measured sweeps: node sizes are added into the root nodes' words; the
-//     CTAs' partials (top two, energy, magnetization, clusters, wraps) are
-//     combined after a fourth barrier and fifth barrier by every CTA, and the
-//     last CTA to finish the |M_C| partials writes the record and the bin
-//     sums (an atomic ticket, no waiting).
+//  5. measured sweeps: node sizes are added into the root nodes' words
+//     (fourth barrier); every CTA's partials (top two, energy,
+//     magnetization, clusters, wraps) are combined by every CTA after a fifth
+//     barrier, the |M_C1|, |M_C2| sums are added up in global memory, and CTA
+//     0 writes the record and the bin sums after the next sweep's first
+//     barrier (or a last barrier at the end of the call), off the critical
+//     path of the sweep.
 //
 // Every load of data another CTA wrote during the launch bypasses L1
 // (ld.global.cg): L1 is not coherent across SMs.  Every wait at a grid
@@ -40,6 +42,33 @@
 #include "rbim_internal.h"
 #include "rbim_open.cuh"
 #include "rbim_tile.cuh"
+
+// Phase profile (profiling builds only, -DRBIM_PROFILE_PHASES): thread 0 of
+// CTA 0 adds the SM cycles since its previous mark to slot k, read and reset
+// with rbim_grid_profile_cycles.
+#ifdef RBIM_PROFILE_PHASES
+__device__ unsigned long long g_grid_phase_cycles[32];
+extern "C" int rbim_grid_profile_cycles(unsigned long long *out, int reset)
+{
+    if (reset) {
+        unsigned long long z[32] = {0};
+        return (int)cudaMemcpyToSymbol(g_grid_phase_cycles, z, sizeof(z));
+    }
+    return (int)cudaMemcpyFromSymbol(out, g_grid_phase_cycles, sizeof(unsigned long long) * 32);
+}
+#define RBIM_GRID_MARK(k)                                                                    \
+    do {                                                                                     \
+        if (blockIdx.x == 0 && threadIdx.x == 0) {                                           \
+            const long long now_ = clock64();                                                \
+            g_grid_phase_cycles[k] += (unsigned long long)(now_ - prof_t);                   \
+            prof_t = now_;                                                                   \
+        }                                                                                    \
+    } while (0)
+#define RBIM_GRID_PROF_START long long prof_t = clock64()
+#else
+#define RBIM_GRID_MARK(k) ((void)0)
+#define RBIM_GRID_PROF_START ((void)0)
+#endif
 
 namespace rbim {
 
@@ -58,11 +87,13 @@ __host__ __device__ constexpr size_t g256(size_t v) { return (v + 255) & ~size_t
 // Shared-memory layout of one CTA's tile for an L x L lattice split in C
 // tiles.
 struct GridLayout {
-    uint32_t L, C, t_max, tw, rows_max, node_max;
-    size_t off_uf, off_S, off_OH, off_OV, off_FLIP, off_ROOT, off_NODE, off_YS, off_NK, off_NR, bytes;
+    uint32_t L, C, t_max, tw, rows_max, node_max, bh;
+    size_t off_uf, off_S, off_OH, off_OV, off_FLIP, off_ROOT, off_NODE, off_YS, off_NK, off_NR, off_BH, bytes;
 };
 
-GridLayout grid_layout(uint32_t L, uint32_t C)
+// with_hash: room for the boundary-bond hash (bh entries, a power of two at
+// least 1.5 times the tile's boundary bonds); without it bh = 0.
+GridLayout grid_layout(uint32_t L, uint32_t C, bool with_hash)
 {
     GridLayout ly{};
     ly.L = L;
@@ -95,24 +126,37 @@ GridLayout grid_layout(uint32_t L, uint32_t C)
     off = g16(off + 4ull * ly.node_max);
     ly.off_NR = off;  // node list: root node (global site) after the boundary stage
     off = g16(off + 4ull * ly.node_max);
+    ly.bh = 0;
+    if (with_hash) {
+        const uint32_t items = L + 1u + ly.rows_max;
+        ly.bh = 64;
+        while (ly.bh < items + items / 2u) ly.bh *= 2u;
+    }
+    ly.off_BH = off;  // boundary-bond hash: (tile root, node, seam crossing) of the bonds unioned
+    off = g16(off + 8ull * ly.bh);
     ly.bytes = off;
     return ly;
 }
 
 namespace {
 
-// Grid-wide barrier state and the record ticket (zeroed before every launch).
+// Grid-wide barrier state (zeroed before every launch): the arrival counter
+// and the abort flag on separate 128-byte lines, and the |M_C1|, |M_C2| sums
+// of the last two measured sweeps (by sweep parity).
 struct GridSync {
-    unsigned int count, gen, ticket;
+    unsigned int count;  // arrivals, never reset within a launch
+    unsigned int pad0[31];
     int abort;
+    unsigned int pad1[31];
+    int mc[2][2];
 };
 
 // One CTA's partial results of a measured sweep.
 struct __align__(16) GridPartial {
     unsigned long long k1, k2;
     uint32_t unsat, downs, ncl;
-    int wrap, mc, mc2;
-    uint32_t pad[6];
+    int wrap;
+    uint32_t pad[8];
 };
 
 // Global workspace of a launch (rbim_grid_workspace_bytes).
@@ -164,34 +208,41 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
     return v;
 }
 
+__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int *p, unsigned int v)
+{
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Grid-wide barrier of a cooperative launch (every CTA resident).  Thread 0
-// of each CTA arrives on a counter; the last arrival resets it and advances
-// the generation, the others wait for the generation to move, for at most
-// `wait_cycles` of the SM clock.  A CTA that gives up raises the abort flag
-// and its error bit; from then on no CTA waits, so every CTA reaches the end
-// of the launch.
+// of each CTA arrives with one acquire-release add on a counter that only
+// grows: barrier k is passed when the counter reaches (k + 1) * nblocks, and
+// the last arrival passes at once.  The others wait for that value, for at
+// most `wait_cycles` of the SM clock; a CTA that gives up raises the abort
+// flag and its error bit, and from then on no CTA waits, so every CTA
+// reaches the end of the launch.  The release of the add covers the CTA's
+// writes before the barrier (they precede it through __syncthreads); the
+// acquire of the final load covers the other CTAs' writes.
 __device__ __forceinline__ void grid_sync(GridSync *gs, uint32_t nblocks, long long wait_cycles, int *err)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned int gen = ld_acquire(&gs->gen);
-        __threadfence();
-        if (atomicAdd(&gs->count, 1u) == nblocks - 1u) {
-            gs->count = 0u;
-            __threadfence();
-            atomicAdd(&gs->gen, 1u);
-        } else {
+        const unsigned int old = atom_add_acq_rel(&gs->count, 1u);
+        const unsigned int target = (old / nblocks + 1u) * nblocks;
+        if (old + 1u != target && !*((volatile int *)&gs->abort)) {
             const long long t0 = clock64();
-            while (ld_acquire(&gs->gen) == gen) {
-                if (*((volatile int *)&gs->abort)) break;
-                if (clock64() - t0 > wait_cycles) {
-                    atomicExch(&gs->abort, 1);
-                    atomicOr(err, kErrGridWait);
-                    break;
+            for (uint32_t it = 1; (int)(ld_acquire(&gs->count) - target) < 0; ++it) {
+                if ((it & 255u) == 1u) {  // after the first load, then every 256
+                    if (*((volatile int *)&gs->abort)) break;
+                    if (clock64() - t0 > wait_cycles) {
+                        atomicExch(&gs->abort, 1);
+                        atomicOr(err, kErrGridWait);
+                        break;
+                    }
                 }
             }
         }
-        __threadfence();
     }
     __syncthreads();
 }
@@ -211,39 +262,6 @@ struct GDist {
     __device__ __forceinline__ unsigned long long ld(uint32_t n) const { return __ldcg(G + n); }
     __device__ __forceinline__ void st(uint32_t n, unsigned long long v) const { __stcg(G + n, v); }
 
-    // Root of node n with the summed image offset of the path; root ~0 when
-    // the walk ran past its bound or met an id outside the lattice.
-    __device__ __forceinline__ FindResult find(uint32_t n) const
-    {
-        uint32_t node = n;
-        int ax = 0, ay = 0;
-        unsigned long long w = ld(node);
-        for (uint32_t it = 0;; ++it) {
-            const uint32_t p = Word64::parent(w);
-            if (p == node) break;
-            if (it >= cap || p >= n_sites) {
-                atomicOr(err, kErrFindCap);
-                return {0xFFFFFFFFu, 0, 0};
-            }
-            const unsigned long long wp = ld(p);
-            const uint32_t gp = Word64::parent(wp);
-            if (gp != p && gp < n_sites) {
-                const int nx = Word64::ox(w) + Word64::ox(wp), ny = Word64::oy(w) + Word64::oy(wp);
-                st(node, Word64::make(gp, nx, ny));
-                ax += nx;
-                ay += ny;
-                node = gp;
-                w = ld(node);
-            } else {
-                ax += Word64::ox(w);
-                ay += Word64::oy(w);
-                node = p;
-                w = wp;
-            }
-        }
-        return {node, ax, ay};
-    }
-
     __device__ __forceinline__ uint32_t root_ro(uint32_t n) const
     {
         uint32_t node = n;
@@ -259,33 +277,74 @@ struct GDist {
         return node;
     }
 
-    // Union across a boundary bond a -> b with seam crossing (ex, ey).
+    // One path-halving step of the walk at x (summed image offset ox, oy):
+    // true when x is a root, false after moving x two levels up.  An id
+    // outside the lattice sets `bad` and stops the walk.
+    __device__ __forceinline__ bool hstep(uint32_t &x, int &ox, int &oy, bool &bad) const
+    {
+        const unsigned long long w = ld(x);
+        const uint32_t p = Word64::parent(w);
+        if (p == x) return true;
+        if (p >= n_sites) {
+            bad = true;
+            return true;
+        }
+        const unsigned long long wp = ld(p);
+        const uint32_t gp = Word64::parent(wp);
+        if (gp == p) {
+            ox += Word64::ox(w);
+            oy += Word64::oy(w);
+            x = p;
+            return true;
+        }
+        if (gp >= n_sites) {
+            bad = true;
+            return true;
+        }
+        const int nx = Word64::ox(w) + Word64::ox(wp), ny = Word64::oy(w) + Word64::oy(wp);
+        st(x, Word64::make(gp, nx, ny));
+        ox += nx;
+        oy += ny;
+        x = gp;
+        return false;
+    }
+
+    // Union across a boundary bond a -> b with seam crossing (ex, ey).  Both
+    // endpoint walks advance in the same iteration (their loads overlap);
+    // once both are at roots the larger root is hooked under the smaller with
+    // a CAS that re-checks it is still a root, and a lost race resumes the
+    // walks from where they stand.
     __device__ __forceinline__ void unite(uint32_t a, uint32_t b, int ex, int ey) const
     {
         if (a >= n_sites || b >= n_sites) {
             atomicOr(err, kErrFindCap);
             return;
         }
+        int axa = 0, aya = 0, axb = 0, ayb = 0;
+        bool da = false, db = false, bad = false;
         for (uint32_t it = 0; it < cap; ++it) {
-            const FindResult fa = find(a);
-            const FindResult fb = find(b);
-            if (fa.root == 0xFFFFFFFFu || fb.root == 0xFFFFFFFFu) return;  // error bit set by find
-            if (fa.root == fb.root) {
+            if (!da) da = hstep(a, axa, aya, bad);
+            if (!db) db = hstep(b, axb, ayb, bad);
+            if (bad) {
+                atomicOr(err, kErrFindCap);
+                return;
+            }
+            if (!(da && db)) continue;
+            if (a == b) {
                 int f = 0;
-                if (Word64::nonzero(ex + fb.ax - fa.ax)) f |= 1;
-                if (Word64::nonzero(ey + fb.ay - fa.ay)) f |= 2;
+                if (Word64::nonzero(ex + axb - axa)) f |= 1;
+                if (Word64::nonzero(ey + ayb - aya)) f |= 2;
                 if (f) atomicOr(wrap, f);
                 return;
             }
-            if (fa.root < fb.root) {
-                const unsigned long long expect = Word64::make(fb.root, 0, 0);
-                const unsigned long long v = Word64::make(fa.root, fa.ax - ex - fb.ax, fa.ay - ey - fb.ay);
-                if (atomicCAS(G + fb.root, expect, v) == expect) return;
+            if (a < b) {
+                const unsigned long long expect = Word64::make(b, 0, 0);
+                if (atomicCAS(G + b, expect, Word64::make(a, axa - ex - axb, aya - ey - ayb)) == expect) return;
             } else {
-                const unsigned long long expect = Word64::make(fa.root, 0, 0);
-                const unsigned long long v = Word64::make(fb.root, fb.ax + ex - fa.ax, fb.ay + ey - fa.ay);
-                if (atomicCAS(G + fa.root, expect, v) == expect) return;
+                const unsigned long long expect = Word64::make(a, 0, 0);
+                if (atomicCAS(G + a, expect, Word64::make(b, axb + ex - axa, ayb + ey - aya)) == expect) return;
             }
+            da = db = false;
         }
         atomicOr(err, kErrUnionCap);
     }
@@ -297,8 +356,10 @@ struct GRed {
     unsigned long long k1[32], k2[32];
     uint32_t unsat[32], downs[32], ncl[32];
     int mcw[32], mcw2[32];
-    uint32_t g1, g2, ncl_total, nnodes, front, tile_end, last;
-    int wrap, err;
+    uint32_t g1, g2, ncl_total, nnodes, front, tile_end, hot_r, hot_s;
+    int wrap, err, pend_many;
+    uint64_t pend_sweep;
+    bool pend;
     long long rec[kRecLen];
     rbim_chain_t ch;
 };
@@ -310,6 +371,7 @@ struct GTile {
     uint32_t *YS;    // occupied y-seam bonds of the rows ending in the tile
     uint32_t *NK;    // node list: tile roots (local sites)
     uint32_t *NR;    // node list: their root nodes (global sites)
+    unsigned long long *BH;  // boundary-bond hash (ly.bh entries, none when 0)
 };
 
 __device__ __forceinline__ GTile make_gtile(unsigned char *smem, const GridLayout &ly, const Tile &tl, GRed &red,
@@ -336,6 +398,7 @@ __device__ __forceinline__ GTile make_gtile(unsigned char *smem, const GridLayou
     x.YS = (uint32_t *)(smem + ly.off_YS);
     x.NK = (uint32_t *)(smem + ly.off_NK);
     x.NR = (uint32_t *)(smem + ly.off_NR);
+    x.BH = (unsigned long long *)(smem + ly.off_BH);
     return x;
 }
 
@@ -430,10 +493,25 @@ __device__ __forceinline__ void grid_nodes(const GTile &x, const Tile &tl, const
 // grid barrier of the sweep).  Lane i of a warp takes item i0 + i, so the
 // x-bonds along the last row sit in consecutive lanes: a bond that joins the
 // same two nodes with the same seam crossing as the previous lane's closes a
-// loop of winding zero (the paths inside tiles do not wrap) and is skipped.
+// loop of winding zero (the paths inside tiles do not wrap) and is skipped,
+// and so is any later such bond of the tile (the boundary-bond hash).
+// First insertion of `key` into the boundary-bond hash (open addressing,
+// mask + 1 slots, never full: it holds at least 1.5 keys per bond).
+__device__ __forceinline__ bool bh_insert(unsigned long long *H, uint32_t mask, unsigned long long key)
+{
+    uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 40) & mask;
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const unsigned long long old = atomicCAS(H + h, ~0ull, key);
+        if (old == ~0ull) return true;
+        if (old == key) return false;
+        h = (h + 1u) & mask;
+    }
+    return true;
+}
+
 template <int NT>
 __device__ __forceinline__ void grid_boundary(const GTile &x, const Tile &tl, const GridWs &ws, const GDist &d,
-                                              uint32_t tile_end, uint32_t tid)
+                                              uint32_t tile_end, uint32_t bh, uint32_t tid)
 {
     const Lat<Word16> &t = x.t;
     const uint32_t rows_end = (tl.b + tl.Tc) / tl.L;  // rows x0 .. rows_end-1 end in the tile
@@ -479,6 +557,12 @@ __device__ __forceinline__ void grid_boundary(const GTile &x, const Tile &tl, co
         const uint32_t pra = __shfl_up_sync(0xFFFFFFFFu, ra, 1), prb = __shfl_up_sync(0xFFFFFFFFu, rb, 1);
         const int ptag = __shfl_up_sync(0xFFFFFFFFu, tag, 1);
         if (live && lane > 0u && ptag == tag && pra == ra && prb == rb) live = false;
+        // Any earlier bond of the tile between the same two nodes with the
+        // same seam crossing makes this one redundant in the same way.
+        if (live && bh)
+            live = bh_insert(x.BH, bh - 1u,
+                             ((unsigned long long)(ra - tl.b) << 34) | ((unsigned long long)rb << 2) |
+                                 (unsigned long long)(ex + 2 * ey));
         if (live) d.unite(ra, rb, ex, ey);
     }
 }
@@ -524,6 +608,58 @@ __device__ __forceinline__ void acc_load_cg(Acc &a, const long long *gi, const d
     a.f[1] = __ldcg(gf + 1);
 }
 
+// The record and bin sums of measured sweep `sw` (warp 0 of CTA 0, after
+// every CTA has finished the sweep): energy, magnetization and wraps from
+// the CTAs' partials, |M_C1| and |M_C2| from the sums the CTAs added for
+// the sweep's parity (reset here for the sweep after next), the cluster
+// count and the two largest sizes from this CTA's own combination.
+__device__ __forceinline__ void grid_record(const GridArgs &a, const rbim_chain_t &ch, GRed &red, uint32_t C,
+                                            uint32_t N, uint32_t lane)
+{
+    const GridWs &ws = a.ws;
+    const uint64_t sw = red.pend_sweep;
+    long long su = 0, sd = 0;
+    int wr = 0;
+    for (uint32_t i = lane; i < C; i += 32u) {
+        su += __ldcg(&ws.part[i].unsat);
+        sd += __ldcg(&ws.part[i].downs);
+        wr |= __ldcg(&ws.part[i].wrap);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        su += __shfl_xor_sync(0xFFFFFFFFu, su, o);
+        sd += __shfl_xor_sync(0xFFFFFFFFu, sd, o);
+        wr |= __shfl_xor_sync(0xFFFFFFFFu, wr, o);
+    }
+    if (lane != 0) return;
+    int *mcs = ws.sync->mc[sw & 1u];
+    const long long m1 = __ldcg(mcs), m2 = __ldcg(mcs + 1);
+    mcs[0] = 0;
+    mcs[1] = 0;
+    long long *rec = red.rec;
+    rec[0] = 2ll * su - 2ll * (long long)N;
+    rec[1] = (long long)N - 2ll * sd;
+    rec[2] = red.ncl_total;
+    const long long mc_total = red.pend_many ? m1 : rec[1], mc2_total = red.pend_many ? m2 : 0;
+    rec[4] = mc_total < 0 ? -mc_total : mc_total;
+    rec[6] = mc2_total < 0 ? -mc2_total : mc2_total;
+    rec[7] = wr & 1;
+    rec[8] = (wr >> 1) & 1;
+    const long long idx = (long long)(sw - (uint64_t)ch.n_therm);
+    const long long bin = idx / ch.sweeps_per_bin;
+    long long *gi = a.acc_i + (ch.acc_off + bin) * kAccInt;
+    double *gf = a.acc_f + (ch.acc_off + bin) * kAccF64;
+    Acc acc;
+    acc_load_cg(acc, gi, gf);
+    acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[7], (int)rec[8]);
+    acc.store(gi, gf);
+    if (a.records && ch.rec_off >= 0) {
+        int32_t *row = a.records + (ch.rec_off + idx) * kRecLen;
+#pragma unroll
+        for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];
+    }
+    red.pend = false;
+}
+
 // One chain, every sweep of the call.  NT threads per CTA, one tile per CTA.
 template <int NT>
 __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(GridArgs a)
@@ -538,6 +674,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
 
     if (tid == 0) {
         red.err = 0;
+        red.pend = false;
         red.ch = *a.chain;
     }
     __syncthreads();
@@ -585,6 +722,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
     uint64_t sweep = ch.sweep;
     const uint64_t stop = min(t_end, sweep + (uint64_t)max(a.n_sweeps, 0));
     const bool second = a.records && ch.rec_off >= 0;
+    RBIM_GRID_PROF_START;
     for (; sweep < stop; ++sweep) {
         const bool measure = sweep >= (uint64_t)ch.n_therm;
         const uint32_t front = red.front;
@@ -595,23 +733,35 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         }
         for (uint32_t i = tid; i < ly.rows_max / 32u + 1u; i += NT) x.YS[i] = 0u;
         for (uint32_t w = tid; w < t.g.NW; w += NT) x.NODE[w] = 0u;
+        for (uint32_t i = tid; i < ly.bh; i += NT) x.BH[i] = ~0ull;
         __syncthreads();
         tile_activate<NT>(t, x.YS, tl, make_rng(ch.key, sweep, ch.thr), gJH, gJV, front, red.tile_end, warp, nwarps,
                           tid);
         __syncthreads();
+        RBIM_GRID_MARK(0);
         for (uint32_t w = tid; w < t.g.NW; w += NT) ws.FLIPG[(tl.b >> 5) + w] = t.FLIP[w];
         phase_heads<Word16>(t, warp, nwarps);
         for (uint32_t w = tid; w < t.g.NW; w += NT) t.ROOT[w] = 0u;
         __syncthreads();
+        RBIM_GRID_MARK(1);
         grid_union<NT>(t, tid);
         __syncthreads();
+        RBIM_GRID_MARK(2);
         grid_roots<NT>(t, tid);
         __syncthreads();
+        RBIM_GRID_MARK(3);
         grid_nodes<NT>(x, tl, ws, red, tid);
+        RBIM_GRID_MARK(4);
         grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // nodes, FR, FRONT and FLIPG are published
+        RBIM_GRID_MARK(5);
+        // Every CTA has finished the previous sweep: its record, off the
+        // critical path of that sweep.
+        if (c == 0 && warp == 0 && red.pend) grid_record(a, ch, red, C, tl.N, lane);
 
-        grid_boundary<NT>(x, tl, ws, d, red.tile_end, tid);
+        grid_boundary<NT>(x, tl, ws, d, red.tile_end, ly.bh, tid);
+        RBIM_GRID_MARK(6);
         grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // every boundary union is done
+        RBIM_GRID_MARK(7);
 
         // Root node of each node; a merged tile root takes the raw flip bit
         // of its cluster's root site.
@@ -630,12 +780,16 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         __syncthreads();
         // Flip run pieces by their tile root's FLIP bit; a measured sweep
         // also leaves every piece leader's word holding its tile root.
+        RBIM_GRID_MARK(8);
         flip_pieces(t, tid, NT, measure);
         __syncthreads();
+        RBIM_GRID_MARK(9);
         for (uint32_t w = tid; w < tl.tw; w += NT) gS[w] = t.S[w] & t.g.valid(w);
         grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // every tile's spins are written
+        RBIM_GRID_MARK(10);
         grid_halo<NT>(x, tl, spins, red, tid);
         __syncthreads();
+        RBIM_GRID_MARK(11);
 
         if (!measure) continue;
 
@@ -655,16 +809,42 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         // may hold all 65536 sites).
         count_pieces<true>(t, u16, warp, nwarps);
         __syncthreads();
+        RBIM_GRID_MARK(12);
         // Node sizes into the root nodes' words (the high half of a root's
-        // word is zero); clusters: tile-only roots and root nodes.
+        // word is zero), summed per root in each warp first and, for the root
+        // of the CTA's first node (most often the cluster that spans the
+        // lattice), over the whole CTA, so that a spanning cluster's root
+        // takes one add per CTA.  Clusters: tile-only roots and root nodes.
+        if (tid == 0) {
+            red.hot_r = nnodes ? x.NR[0] : 0xFFFFFFFFu;
+            red.hot_s = 0u;
+        }
+        __syncthreads();
+        const uint32_t hot = red.hot_r;
         uint32_t nloc = 0;
-        for (uint32_t k = tid; k < nnodes; k += NT) {
-            const uint32_t m = x.NK[k], r = x.NR[k];
-            atomicAdd((unsigned int *)(ws.G + r) + 1, (unsigned int)u16[m] + 1u);
-            if (r == tl.b + m) ++nloc;
+        for (uint32_t k0 = warp << 5; k0 < nnodes; k0 += NT) {
+            const uint32_t k = k0 + lane;
+            uint32_t r = 0xFFFFFFFFu, v = 0u;
+            if (k < nnodes) {
+                const uint32_t m = x.NK[k];
+                r = x.NR[k];
+                v = (uint32_t)u16[m] + 1u;
+                if (r == tl.b + m) ++nloc;
+            }
+            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, r);
+            const uint32_t sum = __reduce_add_sync(grp, v);
+            if (r != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(grp) - 1)) {
+                if (r == hot)
+                    atomicAdd(&red.hot_s, sum);
+                else
+                    atomicAdd((unsigned int *)(ws.G + r) + 1, sum);
+            }
         }
         for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~x.NODE[w]);
+        __syncthreads();
+        if (tid == 0 && hot != 0xFFFFFFFFu) atomicAdd((unsigned int *)(ws.G + hot) + 1, red.hot_s);
         grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // merged sizes are complete
+        RBIM_GRID_MARK(13);
 
         // Local top two: tile-only clusters and the root nodes in this tile.
         unsigned long long k1 = 0, k2 = 0;
@@ -719,6 +899,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
             }
         }
         grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // partials are visible
+        RBIM_GRID_MARK(14);
 
         // Every CTA combines the partials: the two largest clusters and the
         // number of clusters.
@@ -803,58 +984,24 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
                 s1 += red.mcw[i];
                 s2 += red.mcw2[i];
             }
-            __stcg(&ws.part[c].mc, s1);
-            __stcg(&ws.part[c].mc2, s2);
-            __threadfence();
-            red.last = atomicAdd(&ws.sync->ticket, 1u) == C - 1u ? 1u : 0u;
+            if (many) {
+                atomicAdd(&ws.sync->mc[sweep & 1u][0], s1);
+                if (second) atomicAdd(&ws.sync->mc[sweep & 1u][1], s2);
+            }
+            if (c == 0) {
+                red.pend = true;
+                red.pend_sweep = sweep;
+                red.pend_many = many ? 1 : 0;
+            }
         }
         __syncthreads();
-        if (red.last && warp == 0) {
-            // The last CTA: the record of the sweep and the bin sums.
-            __threadfence();
-            long long su = 0, sd = 0, smc = 0, smc2 = 0;
-            int wr = 0;
-            for (uint32_t i = lane; i < C; i += 32u) {
-                su += __ldcg(&ws.part[i].unsat);
-                sd += __ldcg(&ws.part[i].downs);
-                smc += __ldcg(&ws.part[i].mc);
-                smc2 += __ldcg(&ws.part[i].mc2);
-                wr |= __ldcg(&ws.part[i].wrap);
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                su += __shfl_xor_sync(0xFFFFFFFFu, su, o);
-                sd += __shfl_xor_sync(0xFFFFFFFFu, sd, o);
-                smc += __shfl_xor_sync(0xFFFFFFFFu, smc, o);
-                smc2 += __shfl_xor_sync(0xFFFFFFFFu, smc2, o);
-                wr |= __shfl_xor_sync(0xFFFFFFFFu, wr, o);
-            }
-            if (lane == 0) {
-                ws.sync->ticket = 0u;
-                long long *rec = red.rec;
-                rec[0] = 2ll * su - 2ll * (long long)tl.N;
-                rec[1] = (long long)tl.N - 2ll * sd;
-                rec[2] = red.ncl_total;
-                const long long mc_total = many ? smc : rec[1], mc2_total = many ? smc2 : 0;
-                rec[4] = mc_total < 0 ? -mc_total : mc_total;
-                rec[6] = mc2_total < 0 ? -mc2_total : mc2_total;
-                rec[7] = wr & 1;
-                rec[8] = (wr >> 1) & 1;
-                const long long idx = (long long)(sweep - (uint64_t)ch.n_therm);
-                const long long bin = idx / ch.sweeps_per_bin;
-                long long *gi = a.acc_i + (ch.acc_off + bin) * kAccInt;
-                double *gf = a.acc_f + (ch.acc_off + bin) * kAccF64;
-                Acc acc;
-                acc_load_cg(acc, gi, gf);
-                acc.add(rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], (int)rec[7], (int)rec[8]);
-                acc.store(gi, gf);
-                if (second) {
-                    int32_t *row = a.records + (ch.rec_off + idx) * kRecLen;
-#pragma unroll
-                    for (int k = 0; k < kRecLen; ++k) row[k] = (int32_t)rec[k];
-                }
-                __threadfence();
-            }
-        }
+        RBIM_GRID_MARK(15);
+    }
+    // The record of the call's last sweep, after every CTA has finished it
+    // (the same condition on every CTA: the last sweep was measured).
+    if (stop > ch.sweep && stop - 1u >= (uint64_t)ch.n_therm) {
+        grid_sync(ws.sync, C, a.wait_cycles, &red.err);
+        if (c == 0 && warp == 0 && red.pend) grid_record(a, ch, red, C, tl.N, lane);
     }
     if (c == 0 && tid == 0) a.chain->sweep = stop;
     if (tid == 0 && red.err) atomicOr(a.status, red.err);
@@ -904,15 +1051,25 @@ cudaError_t grid_launch_t(const GridArgs &a, uint32_t C, size_t smem, cudaStream
 
 }  // namespace
 
-bool grid_plan_ok(uint32_t L, GridPlan p)
+// The layout a plan runs with: with the boundary-bond hash when it fits in
+// shared memory, else without (false: the plan cannot run an L x L lattice).
+static bool grid_fit(uint32_t L, GridPlan p, GridLayout *out)
 {
     if (L <= 32u || p.C < 2u || (p.threads != 256u && p.threads != 512u && p.threads != 1024u)) return false;
     if ((uint64_t)L * L >= (1ull << 31)) return false;
     if (!cluster_tiles_ok(L, p.C, kGridTileMax)) return false;
-    const GridLayout ly = grid_layout(L, p.C);
     const uint32_t per_sm = 1024u / p.threads;  // register budget: 64 per thread
-    return per_sm * (ly.bytes + kGridStaticSmem) <= kGridSmemPerSm && ly.bytes <= 227u * 1024u - kGridStaticSmem;
+    for (const bool hash : {true, false}) {
+        const GridLayout ly = grid_layout(L, p.C, hash);
+        if (per_sm * (ly.bytes + kGridStaticSmem) <= kGridSmemPerSm && ly.bytes <= 227u * 1024u - kGridStaticSmem) {
+            if (out) *out = ly;
+            return true;
+        }
+    }
+    return false;
 }
+
+bool grid_plan_ok(uint32_t L, GridPlan p) { return grid_fit(L, p, nullptr); }
 
 GridPlan grid_plan(uint32_t L)
 {
@@ -931,8 +1088,8 @@ cudaError_t launch_grid_sweeps(rbim_chain_t *chain, int64_t L, GridPlan plan, ui
                                const uint32_t *coupling_pool, long long *acc_i, double *acc_f, int32_t *records,
                                int n_sweeps, int *status, void *workspace, long long wait_cycles, cudaStream_t stream)
 {
-    if (!grid_plan_ok((uint32_t)L, plan)) return cudaErrorInvalidValue;
     GridArgs a;
+    if (!grid_fit((uint32_t)L, plan, &a.ly)) return cudaErrorInvalidValue;
     a.chain = chain;
     a.spin_pool = spin_pool;
     a.coupling_pool = coupling_pool;
@@ -943,7 +1100,6 @@ cudaError_t launch_grid_sweeps(rbim_chain_t *chain, int64_t L, GridPlan plan, ui
     a.L = L;
     a.status = status;
     a.ws = grid_ws(workspace, (uint32_t)L, plan.C);
-    a.ly = grid_layout((uint32_t)L, plan.C);
     a.wait_cycles = wait_cycles > 0 ? wait_cycles : kGridWaitCycles;
     int per_sm = 0;
     cudaError_t e = grid_occupancy(plan.threads, a.ly.bytes, &per_sm);
