@@ -247,14 +247,16 @@ def run_reference(args, L, ps, n_real, temps):
 # ---------------------------------------------------------------------------
 # GPU legs.
 # ---------------------------------------------------------------------------
-def time_sweeps(cs, n, plain=False, concurrent=True):
+def time_sweeps(cs, n, plain=False, concurrent=True, grid=False):
     """Device time of n sweeps of every chain of a ChainSet (CUDA events on the current stream)."""
     import torch
 
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    if plain:
+    if grid:
+        cs.run_grid(n)
+    elif plain:
         cs.run_plain(n)
     else:
         cs.run_batched(n, concurrent=concurrent)
@@ -266,25 +268,32 @@ def time_sweeps(cs, n, plain=False, concurrent=True):
 
 def c2_line(rb, dev, seed, sweeps):
     """One L = 1024 lattice (p = 0.10, T = 1.6) for ``sweeps`` measured sweeps, and the pure model at T_c, on the
-    engine ``engine="auto"`` picks for one lattice (the plain engine), device-timed; with E/N and <|m|>."""
+    engine ``engine="auto"`` picks for one lattice (the grid engine), device-timed, with E/N and <|m|>; the same
+    runs on the plain engine beside it (its launch sequence replayed as a CUDA graph)."""
     out = {}
     L = 1024
     tc = 2.0 / np.log(1.0 + np.sqrt(2.0))
     for name, p, T in (("p0.10_T1.6", 0.10, 1.6), ("p0_Tc", 0.0, tc)):
         specs, couplings = build_chains(rb, L, [p], 1, [T], seed, sweeps)
-        assert rb.engine.auto_engine(specs) == "plain"
-        cs = rb.ChainSet(specs, couplings, device=dev)
-        cs.init_spins(hot=True)
-        cs.capture_plain(sweeps)  # the launch sequence as a CUDA graph, outside the timed region
-        t = time_sweeps(cs, sweeps, plain=True)
-        ib, _ = cs.bins(0)
+        assert rb.engine.auto_engine(specs) == "grid"
+        res = {}
+        for engine in ("grid", "plain"):
+            cs = rb.ChainSet(specs, couplings, device=dev)
+            cs.init_spins(hot=True)
+            if engine == "plain":
+                cs.capture_plain(sweeps)  # the launch sequence as a CUDA graph, outside the timed region
+            res[engine] = (time_sweeps(cs, sweeps, plain=engine == "plain", grid=engine == "grid"), cs.bins(0)[0])
+        t, ib = res["grid"]
+        assert np.array_equal(ib, res["plain"][1])  # same chain, same sums on both engines
         n = L * L
         out[name] = {"p": p, "T": float(T), "sweeps": sweeps, "device_s": t, "lattice_sweeps_per_s": sweeps / t,
                      "site_updates_per_s": sweeps * n / t, "us_per_sweep": 1e6 * t / sweeps,
+                     "plain_us_per_sweep": 1e6 * res["plain"][0] / sweeps,
+                     "grid_over_plain": res["plain"][0] / t,
                      "E_per_site": float(ib[0, 0]) / sweeps / n, "abs_m": float(ib[0, 3]) / sweeps / n,
                      "S1_over_N": float(ib[0, 5]) / sweeps / n}
-    out["engine"] = "plain (engine='auto' for one lattice with L > 56)"
-    out["note"] = "2,000 measured sweeps from a hot start, no thermalisation excluded"
+    out["engine"] = "grid (engine='auto' for one lattice with L > 32: one cooperative launch per call, tiles on every SM)"
+    out["note"] = "2,000 measured sweeps from a hot start, no thermalisation excluded; bin sums equal on both engines"
     return out
 
 
@@ -576,9 +585,16 @@ def main():
         pcs.capture_plain(args.plain_sweeps)
         torch.cuda.synchronize()
         plain_v = args.plain_sweeps / time_sweeps(pcs, args.plain_sweeps, plain=True)
+        gcs = rb.ChainSet([pspec], [couplings[0]], device=dev)
+        gcs.init_spins(hot=True)
+        gcs.run_grid(10)
+        torch.cuda.synchronize()
+        grid_v = args.plain_sweeps / time_sweeps(gcs, args.plain_sweeps, grid=True)
         plain = {"value": plain_v, "unit": "lattice-sweeps/s",
                  "engine": "plain (global-memory, 7 launches per sweep replayed as a CUDA graph)",
-                 "batched_over_plain": value / world / plain_v}
+                 "batched_over_plain": value / world / plain_v,
+                 "grid_value": grid_v,
+                 "grid_engine": "grid (one cooperative launch per call, the lattice in tiles on every SM)"}
 
     # End to end through the public API: one run_temperature_scan per p per step.
     e2e = None

@@ -209,7 +209,7 @@ def build_parser() -> argparse.ArgumentParser:
     r.add_argument("--disorder-glob", type=str, default=None)
     r.add_argument("--out", type=str, required=True)
     r.add_argument("--backend", choices=["cuda"], default="cuda")
-    r.add_argument("--engine", choices=["auto", "batched", "plain"], default="auto")
+    r.add_argument("--engine", choices=["auto", "batched", "plain", "grid"], default="auto")
     r.add_argument("--chunk", type=int, default=1000, help="sweeps per engine call")
     r.set_defaults(func=run_sweep)
 

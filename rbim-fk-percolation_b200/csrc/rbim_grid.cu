@@ -778,10 +778,16 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
             }
         }
         __syncthreads();
-        // Flip run pieces by their tile root's FLIP bit; a measured sweep
-        // also leaves every piece leader's word holding its tile root.
+        // Flip by the tile root's FLIP bit: run piece by run piece (a
+        // measured sweep also leaves every piece leader's word holding its
+        // tile root), or, in tiles with fewer than a quarter as many words as
+        // threads, site by site (every site's word then holds its tile root).
         RBIM_GRID_MARK(8);
-        flip_pieces(t, tid, NT, measure);
+        const bool per_site = 4u * t.g.NW <= NT;
+        if (!per_site)
+            flip_pieces(t, tid, NT, measure);
+        else
+            phase_sites<Word16>(t, warp, nwarps, true, false);
         __syncthreads();
         RBIM_GRID_MARK(9);
         for (uint32_t w = tid; w < tl.tw; w += NT) gS[w] = t.S[w] & t.g.valid(w);
@@ -950,8 +956,19 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
             }
             __syncthreads();
             // One lane per word, one test per run piece: a piece leader's
-            // word holds its tile root.
-            for (uint32_t w = tid; w < t.g.NW; w += NT) {
+            // word holds its tile root; site by site (one warp per word)
+            // where the flip went site by site.
+            if (per_site) {
+                for (uint32_t w = warp; w < t.g.NW; w += nwarps) {
+                    const uint32_t n = (w << 5) + lane;
+                    if (n >= tl.Tc) continue;
+                    const uint32_t r = ((t.ROOT[w] >> lane) & 1u) ? n : (uint32_t)u16[n];
+                    const int m = 1 - 2 * (int)((t.S[w] >> lane) & 1u);
+                    if ((t.OH[r >> 5] >> (r & 31u)) & 1u) mc += m;
+                    if (second && ((t.FLIP[r >> 5] >> (r & 31u)) & 1u)) mc2 += m;
+                }
+            }
+            for (uint32_t w = tid; w < t.g.NW && !per_site; w += NT) {
                 const uint32_t valid = t.g.valid(w);
                 uint32_t lead = piece_leaders(t, w, valid);
                 const uint32_t roots = t.ROOT[w], sw = t.S[w];

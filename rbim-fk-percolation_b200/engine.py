@@ -22,22 +22,32 @@ import numpy as np
 from . import _native
 from .packing import threshold, unpack_spins, words_for
 
-__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "PLAIN_SINGLE_MIN_L", "auto_engine", "Launch",
+__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "GRID_SINGLE_MIN_L", "PLAIN_SINGLE_MIN_L", "auto_engine", "Launch",
            "launch_buckets"]
 
-#: A set of one lattice runs on the plain engine under ``engine="auto"`` when
-#: its L exceeds this.  Measured on B200 with the plain engine's launch
-#: sequence replayed as a CUDA graph: one resident CTA is faster at L = 48
-#: (20.8 k against 18.5 k sweeps/s), the plain engine from L = 64 up (20.1 k
-#: against 18.9 k at L = 64, 18.9 k against 16.0 k at L = 128).
+#: A set of one lattice runs over the whole GPU under ``engine="auto"``: on
+#: the grid engine when L exceeds GRID_SINGLE_MIN_L and the grid engine has a
+#: plan for L (measured on B200, one lattice: 31.8 us per sweep against
+#: 33.4 us on one resident CTA at L = 40, 32.9 against 47.6 at L = 48), else
+#: on the plain engine when L exceeds PLAIN_SINGLE_MIN_L (one resident CTA is
+#: faster at L = 48, 20.8 k sweeps/s against 18.5 k, the plain engine from
+#: L = 64 up).  Smaller lattices run on one resident CTA.
+GRID_SINGLE_MIN_L = 32
 PLAIN_SINGLE_MIN_L = 56
 
 
-def auto_engine(specs) -> str:
-    """The engine ``engine="auto"`` picks for a set of chains: ``"plain"`` for one lattice with
-    L > PLAIN_SINGLE_MIN_L (the whole grid on one lattice beats one CTA or one cluster), else ``"batched"``."""
+def auto_engine(specs, grid_plan=None) -> str:
+    """The engine ``engine="auto"`` picks for a set of chains.  One lattice: ``"grid"`` (one cooperative launch
+    of tiles over every SM) when L > GRID_SINGLE_MIN_L and the grid engine has a plan for L on the current
+    device, else ``"plain"`` when L > PLAIN_SINGLE_MIN_L, else ``"batched"``; ``"batched"`` for every other set.
+    ``grid_plan(L)`` returns the plan or None (default: ``_native.grid_plan``)."""
     specs = list(specs)
-    return "plain" if len(specs) == 1 and specs[0].L > PLAIN_SINGLE_MIN_L else "batched"
+    if len(specs) != 1:
+        return "batched"
+    L = specs[0].L
+    if L > GRID_SINGLE_MIN_L and (grid_plan or _native.grid_plan)(L):
+        return "grid"
+    return "plain" if L > PLAIN_SINGLE_MIN_L else "batched"
 
 
 def _torch():
@@ -536,12 +546,13 @@ class ChainSet:
     def run_to_end(self, engine: str = "auto", chunk: int = 1000, threads: int = 0) -> None:
         """Run every chain to the end of its run in chunks of ``chunk`` sweeps.
 
-        ``engine="auto"`` runs a set of one lattice with L > PLAIN_SINGLE_MIN_L
-        on the plain engine, whose whole grid works on the one lattice (on
-        B200 a sweep of one L = 256 lattice takes 60 us there against 160 us
-        on one resident CTA, L = 1024 150 us against 200 us on one 16-CTA
-        cluster), and any other set on the batched engines.  Results are the
-        same either way.
+        ``engine="auto"`` (``auto_engine``) runs a set of one lattice over
+        the whole GPU -- on the grid engine where it has a plan (L > 32), else
+        on the plain engine above L = 56 -- and any other set on the batched
+        engines.  On B200 a sweep of one L = 256 lattice takes 40 us
+        on the grid engine, 52 us on the plain engine and 160 us on one
+        resident CTA; L = 1024 67 us, 168 us and 200 us on one 16-CTA cluster.
+        Results are the same on every engine.
         """
         if engine == "auto":
             engine = auto_engine(self.specs)

@@ -243,10 +243,11 @@ def run_single_realization(L: int, J: np.ndarray, temperature: float, *, n_sweep
                            engine: str = "auto", device=None) -> RealizationResult:
     """One realization at one temperature on the GPU (reference ``simulation.py:148-242``).
 
-    ``engine``: ``"plain"`` (global-memory engine, one lattice per launch
-    sequence), ``"batched"`` (resident or cluster engine, one CTA or one
-    cluster for the lattice) or ``"auto"`` (plain for L > 56, where the whole
-    grid on one lattice beats one CTA or one cluster; batched otherwise).
+    ``engine``: ``"grid"`` (one cooperative launch per call, the lattice in
+    shared-memory tiles on every SM), ``"plain"`` (global-memory engine, one
+    lattice per launch sequence), ``"batched"`` (resident or cluster engine,
+    one CTA or one cluster for the lattice) or ``"auto"`` (``auto_engine``:
+    grid for L > 32 where it has a plan, plain for larger L, batched below).
     Every engine gives the same result.
     """
     spb = _check_run(n_sweeps, n_bins)

@@ -14,6 +14,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import _native
 from .engine import ChainSet, ChainSpec, _torch, require_cuda
 from .lattice import Lattice
 from .packing import pack_couplings, pack_spins, threshold, words_for
@@ -95,7 +96,7 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
         if rng is None:
             raise ValueError("sw_sweep needs a key or a numpy Generator")
         key = int(rng.integers(0, 2**63, dtype=np.int64))
-    cs, lock = _sweep_chain_set(L, device)
+    cs, lock, grid = _sweep_chain_set(L, device)
     with lock:
         # One chain whose only sweep is `sweep`: measured when n_therm == sweep.
         cs.coupling_pool[: 2 * words_for(L)].copy_(_torch().from_numpy(pack_couplings(J, L).view(np.int32)))
@@ -104,7 +105,10 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
                                  n_therm=sweep if measure else sweep + 1, n_bins=1, sweeps_per_bin=1)
         cs.acc_int.zero_()
         cs.acc_f64.zero_()
-        cs.run_plain(1)
+        if grid:
+            cs.run_grid(1)  # one cooperative launch over every SM
+        else:
+            cs.run_plain(1)
         cs.check_status()
         spins[...] = cs.spins(0).astype(spins.dtype)
         if not measure:
@@ -118,12 +122,13 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
 
 
 _sets_lock = threading.Lock()
-_sets = {}  # (device, L) -> (ChainSet of one chain with a one-row record buffer, its lock)
+_sets = {}  # (device, L) -> (ChainSet of one chain with a one-row record buffer, its lock, grid engine?)
 
 
 def _sweep_chain_set(L: int, device):
     """The device state ``sw_sweep`` reuses for L x L lattices: one chain set per (device, L), created on first
-    use, so that a caller looping over ``sw_sweep`` does not allocate and free device buffers every sweep."""
+    use, so that a caller looping over ``sw_sweep`` does not allocate and free device buffers every sweep, and
+    whether the sweep runs on the grid engine (where it has a plan for L) or the plain engine."""
     dev = require_cuda(device)
     key = (str(dev), int(L))
     with _sets_lock:
@@ -131,6 +136,8 @@ def _sweep_chain_set(L: int, device):
         if entry is None:
             spec = ChainSpec(L=L, realization=0, key=0, beta=1.0, n_therm=0, n_bins=1, sweeps_per_bin=1, records=True)
             cs = ChainSet([spec], [np.zeros(2 * words_for(L), dtype="<u4")], device=dev)
-            entry = (cs, threading.Lock())
+            with _torch().cuda.device(dev):
+                grid = _native.grid_plan(L) is not None
+            entry = (cs, threading.Lock(), grid)
             _sets[key] = entry
         return entry

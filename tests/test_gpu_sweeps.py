@@ -199,14 +199,15 @@ def test_sw_sweep_api_matches_oracle(rb, orc):
         assert np.array_equal(spins, ref.astype(np.int64))
 
 
-@pytest.mark.parametrize("L", [48, 100, 160])
+@pytest.mark.parametrize("L", [24, 48, 100, 160])
 def test_single_realization_engines_agree(rb, L):
-    """run_single_realization gives the same sums on every engine; engine="auto" takes the plain engine for one
-    lattice with L > PLAIN_SINGLE_MIN_L and the resident engine below."""
+    """run_single_realization gives the same sums on every engine; engine="auto" takes the grid engine for one
+    lattice with L > GRID_SINGLE_MIN_L and the resident engine below."""
     J = _couplings(L, 0.08, L)
+    engines = ("auto", "plain", "batched") + (("grid",) if L > rb.engine.GRID_SINGLE_MIN_L else ())
     out = {e: rb.run_single_realization(L, J, 2.1, n_sweeps=24, n_therm=4, n_bins=4, seed=11, engine=e)
-           for e in ("auto", "plain", "batched")}
-    for e in ("plain", "batched"):
+           for e in engines}
+    for e in engines[1:]:
         for k, v in out["auto"].primitives.items():
             assert np.array_equal(np.float64(v).view(np.uint64), np.float64(out[e].primitives[k]).view(np.uint64)), (e, k)
         for k, v in out["auto"].bin_primitives.items():
