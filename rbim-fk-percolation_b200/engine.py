@@ -307,6 +307,7 @@ class ChainSet:
         self._ws = None
         self._pws = None  # plain-engine workspace; captured graphs hold its address
         self._gws = None  # grid-engine workspace
+        self._grid_ok = {}  # L -> the grid engine has a plan for L on this device
         self._graphs = {}  # (sweeps, chain indices) -> torch.cuda.CUDAGraph of run_plain
 
     # -- helpers -----------------------------------------------------------
@@ -412,7 +413,7 @@ class ChainSet:
                                n_sweeps=n_sweeps, status=self.status.data_ptr(), workspace=ws.data_ptr(),
                                workspace_bytes=ws.numel(), concurrent=concurrent)
         if self.plain_only:
-            self.run_plain(n_sweeps, self.plain_only)
+            self.run_whole_gpu(n_sweeps, self.plain_only)
             done = np.ones(self.n, dtype=bool)
             done[self.plain_only] = False
             self._sweep_host[done] = np.minimum(self._sweep_host[done] + n_sweeps, self.n_total[done])
@@ -506,6 +507,23 @@ class ChainSet:
                     self._ptr(self.status), self._stream())
                 _native.check(rc, "rbim_sweeps_plain_noalloc")
                 self._sweep_host[i] = min(self._sweep_host[i] + n_sweeps, self.n_total[i])
+
+    def grid_ok(self, L: int) -> bool:
+        """Whether the grid engine has a plan for an L x L lattice on this set's device (cached per L)."""
+        if L not in self._grid_ok:
+            with _torch().cuda.device(self.device):
+                self._grid_ok[L] = _native.grid_plan(L) is not None
+        return self._grid_ok[L]
+
+    def run_whole_gpu(self, n_sweeps: int, chains: Sequence[int]) -> None:
+        """Advance chains one at a time over the whole GPU: on the grid engine where it has a plan for the
+        chain's L, else on the plain engine (the lattices beyond the on-chip engines' sizes)."""
+        grid = [int(i) for i in chains if self.grid_ok(self.specs[i].L)]
+        plain = [int(i) for i in chains if not self.grid_ok(self.specs[i].L)]
+        if grid:
+            self.run_grid(n_sweeps, grid)
+        if plain:
+            self.run_plain(n_sweeps, plain)
 
     def _grid_workspace(self, L: int, ctas: int):
         nbytes = int(self.lib.rbim_grid_workspace_bytes(int(L), int(ctas)))

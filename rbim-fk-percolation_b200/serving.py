@@ -17,8 +17,9 @@ for the same request alone, bit for bit.
 
 Lattices with L up to ``rbim_resident_max_l()`` run on the resident engine,
 one lattice per CTA; larger ones up to ``rbim_cluster_max_l()`` on the
-cluster engine, one lattice per thread-block cluster; any larger still on the
-plain engine, one chain after the other inside each quantum.
+cluster engine, one lattice per thread-block cluster; any larger still over
+the whole GPU, one chain after the other inside each quantum: on the grid
+engine where it has a plan for L, else on the plain engine.
 """
 
 from __future__ import annotations
@@ -190,7 +191,8 @@ class ScanServer:
             self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
             # One work-queue counter per concurrent bucket launch.
             self.queue_ws = torch.zeros(QUEUE_SLOT * 64, dtype=torch.uint8, device=self.device)
-        self._plain_ws = None
+        self._plain_ws = None  # workspace of the whole-GPU launches (grid or plain engine)
+        self._grid_plans = {}  # L -> the grid engine has a plan for L on the server's device
         self._planner = ThreadPoolExecutor(max_workers=2, thread_name_prefix="rbim-scan-plan")
         self._inbox: "queue.Queue[_Pending]" = queue.Queue()
         self._waiting: List[_Pending] = []
@@ -348,6 +350,13 @@ class ScanServer:
                                         words, r_off, chains * plan.n_bins, desc, n_total, staged=(staged, d)))
             n_chains += chains
 
+    def _grid_ok(self, L: int) -> bool:
+        """Whether the grid engine has a plan for an L x L lattice on the server's device (cached per L)."""
+        if L not in self._grid_plans:
+            with _torch().cuda.device(self.device):
+                self._grid_plans[L] = _native.grid_plan(L) is not None
+        return self._grid_plans[L]
+
     def _launch(self) -> None:
         """One quantum of sweeps for every admitted chain."""
         torch = _torch()
@@ -402,14 +411,20 @@ class ScanServer:
                            workspace_bytes=self.queue_ws.numel())
             self.launches += len(on_chip)
             if plain:
-                need = max(int(self.lib.rbim_plain_workspace_bytes(L)) for L, _ in plain)
+                need = max(int(self.lib.rbim_plain_workspace_bytes(L)) if not self._grid_ok(L)
+                           else int(self.lib.rbim_grid_workspace_bytes(L, 0)) for L, _ in plain)
                 if self._plain_ws is None or self._plain_ws.numel() < need:
                     self._plain_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+                wsp, wsn = ctypes.c_void_p(self._plain_ws.data_ptr()), self._plain_ws.numel()
                 for L, ptr in plain:
-                    rc = self.lib.rbim_sweeps_plain(L, ctypes.c_void_p(ptr), pool, pool, ai, af, None, self.quantum,
-                                                    st, ctypes.c_void_p(self._plain_ws.data_ptr()),
-                                                    self._plain_ws.numel(), sp)
-                    _native.check(rc, "rbim_sweeps_plain")
+                    if self._grid_ok(L):
+                        rc = self.lib.rbim_sweeps_grid(L, ctypes.c_void_p(ptr), pool, pool, ai, af, None,
+                                                       self.quantum, st, 0, 0, 0, wsp, wsn, sp)
+                        _native.check(rc, "rbim_sweeps_grid")
+                    else:
+                        rc = self.lib.rbim_sweeps_plain(L, ctypes.c_void_p(ptr), pool, pool, ai, af, None,
+                                                        self.quantum, st, wsp, wsn, sp)
+                        _native.check(rc, "rbim_sweeps_plain")
                     self.launches += 1
         finished = []
         for a in live:

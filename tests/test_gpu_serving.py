@@ -64,3 +64,16 @@ def test_oversize_request_is_rejected(rb):
     server = rb.ScanServer(memory_bytes=1 << 20)
     with pytest.raises(ValueError):
         server.submit(rb.ScanRequest(L=256, p=0.1, temperatures=np.linspace(1, 3, 64), n_realizations=64))
+
+
+def test_request_beyond_cluster_sizes_equals_alone(rb):
+    """A request whose lattices exceed the cluster engine's sizes is served over the whole GPU (grid engine),
+    inside the quanta of the mix, with the stand-alone result."""
+    big = rb._native.cluster_max_l() + 40
+    reqs = [dict(L=big, p=0.10, temperatures=[1.6, 2.3], n_realizations=1, n_sweeps=24, n_bins=3, seed=8),
+            dict(L=32, p=0.05, temperatures=[2.0, 2.4], n_realizations=3, n_sweeps=60, n_bins=3, seed=9)]
+    alone = [rb.run_temperature_scan(**r) for r in reqs]
+    with rb.ScanServer(memory_bytes=256 << 20, quantum=10) as server:
+        results = [f.result(timeout=600) for f in [server.submit(rb.ScanRequest(**r)) for r in reqs]]
+    for got, want in zip(results, alone):
+        _assert_same(got, want)

@@ -257,3 +257,11 @@ def test_sw_sweep_reused_state_does_not_leak(rb, orc):
                         res.second_abs_magnetization) == (r[0], r[1], r[2], r[3], r[5], r[6])
             else:
                 assert res is None
+
+
+def test_batched_set_beyond_cluster_sizes_runs_on_whole_gpu(rb, orc):
+    """A batched set whose largest lattice exceeds the cluster engine's sizes runs that lattice over the whole
+    GPU (grid engine) after the on-chip launches; every chain still equals the oracle's."""
+    big = rb._native.cluster_max_l() + 40
+    cs, specs, _ = _chain(rb, orc, [48, big, 96], "batched", n_therm=1, n_bins=1, spb=2, temps=(1.6, 2.269, 3.0))
+    assert [specs[i].L for i in cs.plain_only] == [big] and cs.grid_ok(big)
