@@ -27,8 +27,8 @@ __all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "GRID_SINGLE_MI
 
 #: A set of one lattice runs over the whole GPU under ``engine="auto"``: on
 #: the grid engine when L exceeds GRID_SINGLE_MIN_L and the grid engine has a
-#: plan for L (measured on B200, one lattice: 31.8 us per sweep against
-#: 33.4 us on one resident CTA at L = 40, 32.9 against 47.6 at L = 48), else
+#: plan for L (measured on B200, one lattice: 29.0 us per sweep against
+#: 33.4 us on one resident CTA at L = 40, 29.1 against 47.7 at L = 48), else
 #: on the plain engine when L exceeds PLAIN_SINGLE_MIN_L (one resident CTA is
 #: faster at L = 48, 20.8 k sweeps/s against 18.5 k, the plain engine from
 #: L = 64 up).  Smaller lattices run on one resident CTA.
@@ -568,8 +568,8 @@ class ChainSet:
         the whole GPU -- on the grid engine where it has a plan (L > 32), else
         on the plain engine above L = 56 -- and any other set on the batched
         engines.  On B200 a sweep of one L = 256 lattice takes 40 us
-        on the grid engine, 52 us on the plain engine and 160 us on one
-        resident CTA; L = 1024 67 us, 168 us and 200 us on one 16-CTA cluster.
+        on the grid engine, 56 us on the plain engine and 158 us on one
+        resident CTA; L = 1024 66 us, 160 us and 189 us on one 16-CTA cluster.
         Results are the same on every engine.
         """
         if engine == "auto":
