@@ -22,14 +22,13 @@
 //     around the torus (src/rbim/_unionfind.py:104-124);
 //  4. after a second barrier every node finds its root and takes the root's
 //     raw flip bit (published before the first barrier); the tile flips by
-//     run pieces and writes its spins back; a third barrier;
-//  5. measured sweeps: node sizes are added into the root nodes' words
-//     (fourth barrier); every CTA's partials (top two, energy,
-//     magnetization, clusters, wraps) are combined by every CTA after a fifth
-//     barrier, the |M_C1|, |M_C2| sums are added up in global memory, and CTA
-//     0 writes the record and the bin sums after the next sweep's first
-//     barrier (or a last barrier at the end of the call), off the critical
-//     path of the sweep.
+//     run pieces and writes its spins back (measured sweeps also add their
+//     cluster sizes into the root nodes' words); a third barrier;
+//  5. measured sweeps: every CTA's partials (top two, energy, magnetization,
+//     clusters, wraps) are combined by every CTA after a fourth barrier, the
+//     |M_C1|, |M_C2| sums are added up in global memory, and CTA 0 writes the
+//     record and the bin sums after the next sweep's first barrier (or a last
+//     barrier at the end of the call), off the critical path of the sweep.
 //
 // Every load of data another CTA wrote during the launch bypasses L1
 // (ld.global.cg): L1 is not coherent across SMs.  Every wait at a grid
@@ -791,7 +790,59 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         __syncthreads();
         RBIM_GRID_MARK(9);
         for (uint32_t w = tid; w < tl.tw; w += NT) gS[w] = t.S[w] & t.g.valid(w);
-        grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // every tile's spins are written
+        // Measured sweeps: cluster sizes before the barrier that publishes the
+        // spins, so that one barrier also completes the merged sizes.
+        uint32_t nloc = 0;
+        if (measure) {
+            for (uint32_t w = tid; w < t.g.NW; w += NT) {
+                uint32_t roots = t.ROOT[w];
+                while (roots) {
+                    const uint32_t bb = __ffs(roots) - 1u;
+                    roots &= roots - 1u;
+                    u16[(w << 5) + bb] = 0;
+                }
+            }
+            __syncthreads();
+            // Tile piece sizes minus one into the tile roots' words (a tile piece
+            // may hold all 65536 sites).
+            count_pieces<true>(t, u16, warp, nwarps);
+            __syncthreads();
+            RBIM_GRID_MARK(12);
+            // Node sizes into the root nodes' words (the high half of a root's
+            // word is zero), summed per root in each warp first and, for the root
+            // of the CTA's first node (most often the cluster that spans the
+            // lattice), over the whole CTA, so that a spanning cluster's root
+            // takes one add per CTA.  Clusters: tile-only roots and root nodes.
+            if (tid == 0) {
+                red.hot_r = nnodes ? x.NR[0] : 0xFFFFFFFFu;
+                red.hot_s = 0u;
+            }
+            __syncthreads();
+            const uint32_t hot = red.hot_r;
+            for (uint32_t k0 = warp << 5; k0 < nnodes; k0 += NT) {
+                const uint32_t k = k0 + lane;
+                uint32_t r = 0xFFFFFFFFu, v = 0u;
+                if (k < nnodes) {
+                    const uint32_t m = x.NK[k];
+                    r = x.NR[k];
+                    v = (uint32_t)u16[m] + 1u;
+                    if (r == tl.b + m) ++nloc;
+                }
+                const uint32_t grp = __match_any_sync(0xFFFFFFFFu, r);
+                const uint32_t sum = __reduce_add_sync(grp, v);
+                if (r != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(grp) - 1)) {
+                    if (r == hot)
+                        atomicAdd(&red.hot_s, sum);
+                    else
+                        atomicAdd((unsigned int *)(ws.G + r) + 1, sum);
+                }
+            }
+            for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~x.NODE[w]);
+            __syncthreads();
+            if (tid == 0 && hot != 0xFFFFFFFFu) atomicAdd((unsigned int *)(ws.G + hot) + 1, red.hot_s);
+        }
+        // Every tile's spins are written (and, when measured, every merged size).
+        grid_sync(ws.sync, C, a.wait_cycles, &red.err);
         RBIM_GRID_MARK(10);
         grid_halo<NT>(x, tl, spins, red, tid);
         __syncthreads();
@@ -802,54 +853,6 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         // ---- measurement (reference sw_sweep, src/rbim/swendsen_wang.py:146-172)
         uint32_t unsat = 0, downs = 0;
         tile_energy<NT>(t, tl, gJH, gJV, red.front, tid, unsat, downs);
-        for (uint32_t w = tid; w < t.g.NW; w += NT) {
-            uint32_t roots = t.ROOT[w];
-            while (roots) {
-                const uint32_t bb = __ffs(roots) - 1u;
-                roots &= roots - 1u;
-                u16[(w << 5) + bb] = 0;
-            }
-        }
-        __syncthreads();
-        // Tile piece sizes minus one into the tile roots' words (a tile piece
-        // may hold all 65536 sites).
-        count_pieces<true>(t, u16, warp, nwarps);
-        __syncthreads();
-        RBIM_GRID_MARK(12);
-        // Node sizes into the root nodes' words (the high half of a root's
-        // word is zero), summed per root in each warp first and, for the root
-        // of the CTA's first node (most often the cluster that spans the
-        // lattice), over the whole CTA, so that a spanning cluster's root
-        // takes one add per CTA.  Clusters: tile-only roots and root nodes.
-        if (tid == 0) {
-            red.hot_r = nnodes ? x.NR[0] : 0xFFFFFFFFu;
-            red.hot_s = 0u;
-        }
-        __syncthreads();
-        const uint32_t hot = red.hot_r;
-        uint32_t nloc = 0;
-        for (uint32_t k0 = warp << 5; k0 < nnodes; k0 += NT) {
-            const uint32_t k = k0 + lane;
-            uint32_t r = 0xFFFFFFFFu, v = 0u;
-            if (k < nnodes) {
-                const uint32_t m = x.NK[k];
-                r = x.NR[k];
-                v = (uint32_t)u16[m] + 1u;
-                if (r == tl.b + m) ++nloc;
-            }
-            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, r);
-            const uint32_t sum = __reduce_add_sync(grp, v);
-            if (r != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(grp) - 1)) {
-                if (r == hot)
-                    atomicAdd(&red.hot_s, sum);
-                else
-                    atomicAdd((unsigned int *)(ws.G + r) + 1, sum);
-            }
-        }
-        for (uint32_t w = tid; w < t.g.NW; w += NT) nloc += __popc(t.ROOT[w] & ~x.NODE[w]);
-        __syncthreads();
-        if (tid == 0 && hot != 0xFFFFFFFFu) atomicAdd((unsigned int *)(ws.G + hot) + 1, red.hot_s);
-        grid_sync(ws.sync, C, a.wait_cycles, &red.err);  // merged sizes are complete
         RBIM_GRID_MARK(13);
 
         // Local top two: tile-only clusters and the root nodes in this tile.
