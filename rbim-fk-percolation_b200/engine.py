@@ -22,32 +22,35 @@ import numpy as np
 from . import _native
 from .packing import threshold, unpack_spins, words_for
 
-__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "GRID_SINGLE_MIN_L", "PLAIN_SINGLE_MIN_L", "auto_engine", "Launch",
+__all__ = ["ChainSpec", "ChainSet", "chain_key", "require_cuda", "SINGLE_CTA_MAX_L", "single_cta_threads", "auto_engine", "Launch",
            "launch_buckets"]
 
-#: A set of one lattice runs over the whole GPU under ``engine="auto"``: on
-#: the grid engine when L exceeds GRID_SINGLE_MIN_L and the grid engine has a
-#: plan for L (measured on B200, one lattice: 29.0 us per sweep against
-#: 33.4 us on one resident CTA at L = 40, 29.1 against 47.7 at L = 48), else
-#: on the plain engine when L exceeds PLAIN_SINGLE_MIN_L (one resident CTA is
-#: faster at L = 48, 20.8 k sweeps/s against 18.5 k, the plain engine from
-#: L = 64 up).  Smaller lattices run on one resident CTA.
-GRID_SINGLE_MIN_L = 32
-PLAIN_SINGLE_MIN_L = 56
+#: A set of one lattice runs under ``engine="auto"`` on one resident CTA when
+#: L <= SINGLE_CTA_MAX_L, with the CTA size ``single_cta_threads(L)``, and
+#: over the whole GPU above: on the grid engine where it has a plan for L, else
+#: on the plain engine.  Measured on B200, one lattice, us per sweep: L = 32,
+#: one CTA of 512 threads 16.5 (64 threads, the batch default, 32.7); L = 48,
+#: one CTA of 1024 threads 22.8, grid engine 28.6; L = 64, 26.0 against 29.9;
+#: L = 96, 42.9 against 32.2.
+SINGLE_CTA_MAX_L = 64
+
+
+def single_cta_threads(L: int) -> int:
+    """CTA size for one lattice alone on the resident engine: the large sizes minimise the time per sweep (the
+    batch default favours many CTAs per SM instead).  Measured on B200: 512 threads up to L = 32 (16.1 us at
+    L = 24 and 16.5 at L = 32, against 17.3 with 1024), 1024 above (22.8 us at L = 48 against 25.9 with 512)."""
+    return 512 if L <= 32 else 1024
 
 
 def auto_engine(specs, grid_plan=None) -> str:
-    """The engine ``engine="auto"`` picks for a set of chains.  One lattice: ``"grid"`` (one cooperative launch
-    of tiles over every SM) when L > GRID_SINGLE_MIN_L and the grid engine has a plan for L on the current
-    device, else ``"plain"`` when L > PLAIN_SINGLE_MIN_L, else ``"batched"``; ``"batched"`` for every other set.
+    """The engine ``engine="auto"`` picks for a set of chains: ``"batched"`` for several lattices, or one with
+    L <= SINGLE_CTA_MAX_L (one resident CTA); for one larger lattice ``"grid"`` (one cooperative launch of tiles
+    over every SM) where the grid engine has a plan for L on the current device, else ``"plain"``.
     ``grid_plan(L)`` returns the plan or None (default: ``_native.grid_plan``)."""
     specs = list(specs)
-    if len(specs) != 1:
+    if len(specs) != 1 or specs[0].L <= SINGLE_CTA_MAX_L:
         return "batched"
-    L = specs[0].L
-    if L > GRID_SINGLE_MIN_L and (grid_plan or _native.grid_plan)(L):
-        return "grid"
-    return "plain" if L > PLAIN_SINGLE_MIN_L else "batched"
+    return "grid" if (grid_plan or _native.grid_plan)(specs[0].L) else "plain"
 
 
 def _torch():
@@ -564,16 +567,19 @@ class ChainSet:
     def run_to_end(self, engine: str = "auto", chunk: int = 1000, threads: int = 0) -> None:
         """Run every chain to the end of its run in chunks of ``chunk`` sweeps.
 
-        ``engine="auto"`` (``auto_engine``) runs a set of one lattice over
-        the whole GPU -- on the grid engine where it has a plan (L > 32), else
-        on the plain engine above L = 56 -- and any other set on the batched
-        engines.  On B200 a sweep of one L = 256 lattice takes 40 us
+        ``engine="auto"`` (``auto_engine``) runs a set of one lattice with
+        L <= 64 on one resident CTA of ``single_cta_threads(L)`` threads, one
+        larger lattice over the whole GPU -- on the grid engine where it has a
+        plan, else on the plain engine -- and any other set on the batched
+        engines.  On B200 a sweep of one L = 256 lattice takes 38 us
         on the grid engine, 56 us on the plain engine and 158 us on one
         resident CTA; L = 1024 66 us, 160 us and 189 us on one 16-CTA cluster.
         Results are the same on every engine.
         """
         if engine == "auto":
             engine = auto_engine(self.specs)
+        if engine == "batched" and threads == 0 and self.n == 1 and self.specs[0].L <= self.lib.rbim_resident_max_l():
+            threads = single_cta_threads(self.specs[0].L)
         if engine not in ("batched", "plain", "grid"):
             raise ValueError(f"engine must be 'auto', 'batched', 'plain' or 'grid', got {engine!r}")
         while self.remaining() > 0:

@@ -14,8 +14,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import _native
-from .engine import ChainSet, ChainSpec, _torch, require_cuda
+from .engine import ChainSet, ChainSpec, _torch, auto_engine, require_cuda, single_cta_threads
 from .lattice import Lattice
 from .packing import pack_couplings, pack_spins, threshold, words_for
 
@@ -96,7 +95,7 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
         if rng is None:
             raise ValueError("sw_sweep needs a key or a numpy Generator")
         key = int(rng.integers(0, 2**63, dtype=np.int64))
-    cs, lock, grid = _sweep_chain_set(L, device)
+    cs, lock, engine = _sweep_chain_set(L, device)
     with lock:
         # One chain whose only sweep is `sweep`: measured when n_therm == sweep.
         cs.coupling_pool[: 2 * words_for(L)].copy_(_torch().from_numpy(pack_couplings(J, L).view(np.int32)))
@@ -105,8 +104,10 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
                                  n_therm=sweep if measure else sweep + 1, n_bins=1, sweeps_per_bin=1)
         cs.acc_int.zero_()
         cs.acc_f64.zero_()
-        if grid:
+        if engine == "grid":
             cs.run_grid(1)  # one cooperative launch over every SM
+        elif engine == "batched":
+            cs.run_batched(1, threads=single_cta_threads(L))  # one resident CTA
         else:
             cs.run_plain(1)
         cs.check_status()
@@ -122,13 +123,13 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
 
 
 _sets_lock = threading.Lock()
-_sets = {}  # (device, L) -> (ChainSet of one chain with a one-row record buffer, its lock, grid engine?)
+_sets = {}  # (device, L) -> (ChainSet of one chain with a one-row record buffer, its lock, engine)
 
 
 def _sweep_chain_set(L: int, device):
     """The device state ``sw_sweep`` reuses for L x L lattices: one chain set per (device, L), created on first
     use, so that a caller looping over ``sw_sweep`` does not allocate and free device buffers every sweep, and
-    whether the sweep runs on the grid engine (where it has a plan for L) or the plain engine."""
+    and the engine the sweep runs on: ``auto_engine``'s choice for one lattice."""
     dev = require_cuda(device)
     key = (str(dev), int(L))
     with _sets_lock:
@@ -137,7 +138,7 @@ def _sweep_chain_set(L: int, device):
             spec = ChainSpec(L=L, realization=0, key=0, beta=1.0, n_therm=0, n_bins=1, sweeps_per_bin=1, records=True)
             cs = ChainSet([spec], [np.zeros(2 * words_for(L), dtype="<u4")], device=dev)
             with _torch().cuda.device(dev):
-                grid = _native.grid_plan(L) is not None
-            entry = (cs, threading.Lock(), grid)
+                engine = auto_engine([spec])
+            entry = (cs, threading.Lock(), engine)
             _sets[key] = entry
         return entry

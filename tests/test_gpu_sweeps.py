@@ -201,10 +201,10 @@ def test_sw_sweep_api_matches_oracle(rb, orc):
 
 @pytest.mark.parametrize("L", [24, 48, 100, 160])
 def test_single_realization_engines_agree(rb, L):
-    """run_single_realization gives the same sums on every engine; engine="auto" takes the grid engine for one
-    lattice with L > GRID_SINGLE_MIN_L and the resident engine below."""
+    """run_single_realization gives the same sums on every engine; engine="auto" takes one resident CTA (of the
+    single-lattice size) for L <= SINGLE_CTA_MAX_L and the grid engine above."""
     J = _couplings(L, 0.08, L)
-    engines = ("auto", "plain", "batched") + (("grid",) if L > rb.engine.GRID_SINGLE_MIN_L else ())
+    engines = ("auto", "plain", "batched") + (("grid",) if L > 32 else ())
     out = {e: rb.run_single_realization(L, J, 2.1, n_sweeps=24, n_therm=4, n_bins=4, seed=11, engine=e)
            for e in engines}
     for e in engines[1:]:

@@ -156,18 +156,18 @@ def test_threshold(rb):
 
 
 def test_auto_engine_choice(rb):
-    """engine="auto", one lattice: the grid engine for L > GRID_SINGLE_MIN_L where it has a plan, else the plain
-    engine for L > PLAIN_SINGLE_MIN_L, else batched; batched for every other set."""
+    """engine="auto", one lattice: one resident CTA for L <= SINGLE_CTA_MAX_L (512 threads up to L = 32, 1024
+    above), else the grid engine where it has a plan, else the plain engine; batched for every other set."""
     eng = rb.engine
     spec = lambda L: rb.ChainSpec(L=L, realization=0, key=1, beta=0.5, n_therm=0, n_bins=1, sweeps_per_bin=1)
-    g, m = eng.GRID_SINGLE_MIN_L, eng.PLAIN_SINGLE_MIN_L
+    m = eng.SINGLE_CTA_MAX_L
     plan = lambda L: (148, 1024) if 32 < L <= 3000 else None
-    assert eng.auto_engine([spec(g + 1)], plan) == "grid" and eng.auto_engine([spec(1024)], plan) == "grid"
-    assert eng.auto_engine([spec(g)], plan) == "batched" and eng.auto_engine([spec(16)], plan) == "batched"
+    assert eng.auto_engine([spec(m + 1)], plan) == "grid" and eng.auto_engine([spec(1024)], plan) == "grid"
+    assert eng.auto_engine([spec(m)], plan) == "batched" and eng.auto_engine([spec(16)], plan) == "batched"
     assert eng.auto_engine([spec(4096)], plan) == "plain"
-    none = lambda L: None
-    assert eng.auto_engine([spec(m + 1)], none) == "plain" and eng.auto_engine([spec(m)], none) == "batched"
+    assert eng.auto_engine([spec(m + 1)], lambda L: None) == "plain"
     assert eng.auto_engine([spec(1024), spec(1024)], plan) == "batched"
+    assert [eng.single_cta_threads(L) for L in (3, 32, 33, 64)] == [512, 512, 1024, 1024]
 
 
 def test_chain_keys_follow_seed_sequences(rb):
