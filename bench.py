@@ -292,7 +292,7 @@ def c2_line(rb, dev, seed, sweeps):
                      "grid_over_plain": res["plain"][0] / t,
                      "E_per_site": float(ib[0, 0]) / sweeps / n, "abs_m": float(ib[0, 3]) / sweeps / n,
                      "S1_over_N": float(ib[0, 5]) / sweeps / n}
-    out["engine"] = "grid (engine='auto' for one lattice with L > 32: one cooperative launch per call, tiles on every SM)"
+    out["engine"] = "grid (engine='auto' for one lattice with L > 64: one cooperative launch per call, tiles on every SM)"
     out["note"] = "2,000 measured sweeps from a hot start, no thermalisation excluded; bin sums equal on both engines"
     return out
 

@@ -247,7 +247,7 @@ def run_single_realization(L: int, J: np.ndarray, temperature: float, *, n_sweep
     shared-memory tiles on every SM), ``"plain"`` (global-memory engine, one
     lattice per launch sequence), ``"batched"`` (resident or cluster engine,
     one CTA or one cluster for the lattice) or ``"auto"`` (``auto_engine``:
-    grid for L > 32 where it has a plan, plain for larger L, batched below).
+    one resident CTA for L <= 64, grid above where it has a plan, else plain).
     Every engine gives the same result.
     """
     spb = _check_run(n_sweeps, n_bins)
