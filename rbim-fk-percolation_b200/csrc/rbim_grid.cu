@@ -1036,21 +1036,42 @@ int device_sm_count()
 }
 
 template <int NT>
-cudaError_t grid_occupancy_t(size_t smem, int *per_sm)
+cudaError_t grid_occupancy_t(size_t smem, bool query, int *per_sm)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_grid_sweeps<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    // The kernel's dynamic shared-memory limit, raised to what any plan may
+    // use, on every launch (a device reset forgets it).
+    const cudaError_t e = cudaFuncSetAttribute(k_grid_sweeps<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(227u * 1024u - kGridStaticSmem));
+    if (e != cudaSuccess || !query) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_grid_sweeps<NT>, NT, smem);
 }
 
+// CTAs of `threads` threads and `smem` dynamic bytes that one SM holds; the
+// query is cached per (device, threads, smem), so that a call of one sweep
+// does not pay for it again.
 cudaError_t grid_occupancy(uint32_t threads, size_t smem, int *per_sm)
 {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<int, uint64_t>, int>> cache;  // (device, threads << 32 | smem) -> CTAs
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t key = ((uint64_t)threads << 32) | (uint64_t)smem;
+    std::lock_guard<std::mutex> lock(mu);
+    bool query = true;
+    for (const auto &c : cache)
+        if (c.first.first == dev && c.first.second == key) {
+            *per_sm = c.second;
+            query = false;
+        }
     switch (threads) {
-    case 256: return grid_occupancy_t<256>(smem, per_sm);
-    case 512: return grid_occupancy_t<512>(smem, per_sm);
-    case 1024: return grid_occupancy_t<1024>(smem, per_sm);
+    case 256: e = grid_occupancy_t<256>(smem, query, per_sm); break;
+    case 512: e = grid_occupancy_t<512>(smem, query, per_sm); break;
+    case 1024: e = grid_occupancy_t<1024>(smem, query, per_sm); break;
     default: return cudaErrorInvalidValue;
     }
+    if (e == cudaSuccess && query) cache.push_back({{dev, key}, *per_sm});
+    return e;
 }
 
 template <int NT>

@@ -16,7 +16,7 @@ import numpy as np
 
 from .engine import ChainSet, ChainSpec, _torch, auto_engine, require_cuda, single_cta_threads
 from .lattice import Lattice
-from .packing import pack_couplings, pack_spins, threshold, words_for
+from .packing import pack_couplings, pack_spins, threshold, unpack_spins, words_for
 
 __all__ = [
     "SweepResult",
@@ -111,7 +111,7 @@ def sw_sweep(spins: np.ndarray, lattice: Lattice, J: np.ndarray, beta: float, rn
         else:
             cs.run_plain(1)
         cs.check_status()
-        spins[...] = cs.spins(0).astype(spins.dtype)
+        spins[...] = unpack_spins(cs.spin_words(0), L, dtype=spins.dtype)
         if not measure:
             return None
         rec = cs.chain_records(0)[0]
