@@ -160,3 +160,13 @@ def test_grid_walk_bound_fires(rb):
     assert st & (FIND_CAP | UNION_CAP), st
     assert not st & (BAD_CHAIN | GRID_WAIT)
     assert cs.device_sweeps()[0] == 3
+
+
+def test_grid_without_boundary_hash(rb, orc):
+    """L = 2800: tiles of about 53,000 sites leave no shared memory for the boundary-bond hash, so every bond the
+    neighbouring-lane filter keeps is unioned globally; the chain is still bit-exact."""
+    cs, spec, J = _chain_set(rb, 2800, 2.269, n_therm=1, n_bins=1, spb=2)
+    assert rb._native.grid_plan(2800) is not None
+    cs.run_grid(3)
+    cs.check_status()
+    _assert_oracle(rb, orc, cs, spec, J)
