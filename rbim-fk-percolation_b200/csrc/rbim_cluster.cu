@@ -324,7 +324,9 @@ struct Dist {
 
 // (b) Boundary bonds owned by this tile: x-bonds of its last L sites, the
 // y-bond from its last site into the next tile, and the y-seam bonds of the
-// rows ending in it.
+// rows ending in it.  Lane i of a warp takes item i0 + i, so the x-bonds along
+// the last row sit in consecutive lanes and repeated pairs of tile roots are
+// dropped before they reach the cluster-wide union-find.
 template <int NT>
 __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, const Dist &d, uint32_t tile_end,
                                               uint32_t tid)
@@ -334,46 +336,65 @@ __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, cons
     const uint32_t n_rows = rows_end - tl.x0;
     const uint32_t items = tl.L + 1u + n_rows;
     const uint32_t nxt = tl.c + 1u == tl.C ? 0u : tl.c + 1u;
-    for (uint32_t i = tid; i < items; i += NT) {
-        uint32_t a, tb, bl;
+    const uint32_t lane = tid & 31u;
+    for (uint32_t i0 = tid & ~31u; i0 < items; i0 += NT) {
+        const uint32_t i = i0 + lane;
+        bool live = false;
+        uint32_t a = 0, tb = 0, bl = 0;
         int ex = 0, ey = 0;
         if (i < tl.L) {
             a = tl.Tc - tl.L + i;
-            if (!((t.OH[a >> 5] >> (a & 31u)) & 1u)) continue;
-            const uint32_t n = tl.b + a;
-            if (n + tl.L >= tl.N) {
-                tb = 0u;
-                bl = n + tl.L - tl.N;
-                ex = 1;
-            } else {
-                tb = nxt;
-                bl = a + tl.L - tl.Tc;
+            if ((t.OH[a >> 5] >> (a & 31u)) & 1u) {
+                live = true;
+                const uint32_t n = tl.b + a;
+                if (n + tl.L >= tl.N) {
+                    tb = 0u;
+                    bl = n + tl.L - tl.N;
+                    ex = 1;
+                } else {
+                    tb = nxt;
+                    bl = a + tl.L - tl.Tc;
+                }
             }
         } else if (i == tl.L) {
-            if (!tile_end) continue;
-            a = tl.Tc - 1u;
-            tb = nxt;
-            bl = 0u;
-        } else {
-            const uint32_t row = i - tl.L - 1u;
-            if (!((x.YS[row >> 5] >> (row & 31u)) & 1u)) continue;
-            const uint32_t xr = tl.x0 + row;
-            a = xr * tl.L + tl.L - 1u - tl.b;
-            const uint32_t start = xr * tl.L;
-            if (start >= tl.b) {
-                tb = tl.c;
-                bl = start - tl.b;
-            } else {
-                tb = tl.c - 1u;
-                bl = start - (tl.b - tl.T);
+            if (tile_end) {
+                live = true;
+                a = tl.Tc - 1u;
+                tb = nxt;
+                bl = 0u;
             }
-            ey = 1;
+        } else if (i < items) {
+            const uint32_t row = i - tl.L - 1u;
+            if ((x.YS[row >> 5] >> (row & 31u)) & 1u) {
+                live = true;
+                const uint32_t xr = tl.x0 + row;
+                a = xr * tl.L + tl.L - 1u - tl.b;
+                const uint32_t start = xr * tl.L;
+                if (start >= tl.b) {
+                    tb = tl.c;
+                    bl = start - tl.b;
+                } else {
+                    tb = tl.c - 1u;
+                    bl = start - (tl.b - tl.T);
+                }
+                ey = 1;
+            }
         }
-        const uint32_t ra = tile_root(t.uf.w, a);
-        const unsigned short *ufb = tb == tl.c ? t.uf.w : d.cl.map_shared_rank(t.uf.w, tb);
-        const uint32_t rb = tile_root(ufb, bl);
+        uint32_t ra = 0, rb = 0;
+        if (live) {
+            ra = tile_root(t.uf.w, a);
+            const unsigned short *ufb = tb == tl.c ? t.uf.w : d.cl.map_shared_rank(t.uf.w, tb);
+            rb = (tb << 16) | tile_root(ufb, bl);
+        }
+        // A bond joining the same two tile roots with the same seam crossing
+        // as the previous lane's closes a loop of winding zero (paths inside a
+        // tile never wrap) and changes nothing.
+        const int tag = live ? 1 + ex + 2 * ey : 0;
+        const uint32_t pra = __shfl_up_sync(0xFFFFFFFFu, ra, 1), prb = __shfl_up_sync(0xFFFFFFFFu, rb, 1);
+        const int ptag = __shfl_up_sync(0xFFFFFFFFu, tag, 1);
+        if (!live || (lane > 0u && ptag == tag && pra == ra && prb == rb)) continue;
         const uint32_t na = d.insert(tl.c, ra);
-        const uint32_t nb = d.insert(tb, rb);
+        const uint32_t nb = d.insert(tb, rb & 0xFFFFu);
         d.unite(na, nb, ex, ey);
     }
 }
