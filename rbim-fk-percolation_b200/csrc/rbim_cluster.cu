@@ -602,17 +602,10 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
             unsigned short *u16 = t.uf.w;
             uint32_t unsat = 0, downs = 0;
             tile_energy<NT>(x.t, tl, gJH, gJV, red.front, tid, unsat, downs);
-            for (uint32_t w = tid; w < t.g.NW; w += NT) {
-                uint32_t roots = t.ROOT[w];
-                while (roots) {
-                    const uint32_t bb = __ffs(roots) - 1u;
-                    roots &= roots - 1u;
-                    u16[(w << 5) + bb] = 0;
-                }
-            }
-            __syncthreads();
-            // Tile piece sizes minus one into the tile roots' words (a tile
-            // piece may hold all 65536 sites).
+            // Tile cluster sizes minus one added onto each tile root's own index
+            // (a root points at itself): afterwards the word of root m reads
+            // m + size - 1, below 65536 because m is the smallest site of its tile
+            // cluster, so no add carries out of its 16 bits (tile_size decodes it).
             count_pieces<true>(t, u16, warp, nwarps);
             __syncthreads();
             // FLIP (no longer needed this sweep) becomes the plane of node
@@ -627,7 +620,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 const uint32_t r = node_root(x, k);
                 atomicOr(t.FLIP + (m >> 5), 1u << (m & 31u));
                 unsigned int *hi = (unsigned int *)(cl.map_shared_rank(x.HW, r >> 16) + (r & 0xFFFFu)) + 1;
-                atomicAdd(hi, (unsigned int)u16[m] + 1u);
+                atomicAdd(hi, tile_size(u16, m));
                 if (r == ((c << 16) | k)) ++rootnodes;
             }
             __syncthreads();
@@ -643,7 +636,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                     const uint32_t bb = __ffs(roots) - 1u;
                     roots &= roots - 1u;
                     const uint32_t m = (w << 5) + bb;
-                    top2_merge(k1, k2, size_key((uint32_t)u16[m] + 1u, tl.b + m), 0ull);
+                    top2_merge(k1, k2, size_key(tile_size(u16, m), tl.b + m), 0ull);
                 }
             }
             for (uint32_t k = tid; k < x.hs; k += NT) {

@@ -794,17 +794,10 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
         // spins, so that one barrier also completes the merged sizes.
         uint32_t nloc = 0;
         if (measure) {
-            for (uint32_t w = tid; w < t.g.NW; w += NT) {
-                uint32_t roots = t.ROOT[w];
-                while (roots) {
-                    const uint32_t bb = __ffs(roots) - 1u;
-                    roots &= roots - 1u;
-                    u16[(w << 5) + bb] = 0;
-                }
-            }
-            __syncthreads();
-            // Tile piece sizes minus one into the tile roots' words (a tile piece
-            // may hold all 65536 sites).
+            // Tile cluster sizes minus one added onto each tile root's own index
+            // (a root points at itself): afterwards the word of root m reads
+            // m + size - 1, below 65536 because m is the smallest site of its tile
+            // cluster, so no add carries out of its 16 bits (tile_size decodes it).
             count_pieces<true>(t, u16, warp, nwarps);
             __syncthreads();
             RBIM_GRID_MARK(12);
@@ -825,7 +818,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
                 if (k < nnodes) {
                     const uint32_t m = x.NK[k];
                     r = x.NR[k];
-                    v = (uint32_t)u16[m] + 1u;
+                    v = tile_size(u16, m);
                     if (r == tl.b + m) ++nloc;
                 }
                 const uint32_t grp = __match_any_sync(0xFFFFFFFFu, r);
@@ -863,7 +856,7 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT) k_grid_sweeps(
                 const uint32_t bb = __ffs(roots) - 1u;
                 roots &= roots - 1u;
                 const uint32_t m = (w << 5) + bb;
-                top2_merge(k1, k2, size_key((uint32_t)u16[m] + 1u, tl.b + m), 0ull);
+                top2_merge(k1, k2, size_key(tile_size(u16, m), tl.b + m), 0ull);
             }
         }
         for (uint32_t k = tid; k < nnodes; k += NT) {

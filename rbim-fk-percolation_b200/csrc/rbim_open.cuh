@@ -278,7 +278,9 @@ __device__ __forceinline__ void add16(unsigned short *base, uint32_t i, uint32_t
 // so a giant cluster sees one add per block instead of one per piece.
 // kMinusOne: the piece that starts at the root adds one less, so that a root
 // word holds size - 1 (a tile of 65536 sites then still fits 16 bits).
-// Root words must be zero on entry.
+// Each root word must hold zero or the root's own index on entry (a root
+// points at itself, so counting onto it needs no zeroing pass; the caller
+// then subtracts the index).
 template <bool kMinusOne>
 __device__ __forceinline__ void count_pieces(const Lat<Word16> &t, unsigned short *u16, uint32_t warp,
                                              uint32_t nwarps)

@@ -168,4 +168,11 @@ __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g
     return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
 }
 
+// Size of the tile cluster of tile root m once the sizes minus one have been
+// added onto the roots' own indices (count_pieces<true> without zeroing).
+__device__ __forceinline__ uint32_t tile_size(const unsigned short *u16, uint32_t m)
+{
+    return (((uint32_t)u16[m] - m) & 0xFFFFu) + 1u;
+}
+
 }  // namespace rbim
