@@ -329,7 +329,7 @@ struct Dist {
 // dropped before they reach the cluster-wide union-find.
 template <int NT>
 __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, const Dist &d, uint32_t tile_end,
-                                              uint32_t tid)
+                                              bool walk, uint32_t tid)
 {
     const Lat<Word16> &t = x.t;
     const uint32_t rows_end = (tl.b + tl.Tc) / tl.L;  // rows x0 .. rows_end-1 end in the tile
@@ -382,9 +382,14 @@ __device__ __forceinline__ void tile_boundary(const Ctx &x, const Tile &tl, cons
         }
         uint32_t ra = 0, rb = 0;
         if (live) {
-            ra = tile_root(t.uf.w, a);
             const unsigned short *ufb = tb == tl.c ? t.uf.w : d.cl.map_shared_rank(t.uf.w, tb);
-            rb = (tb << 16) | tile_root(ufb, bl);
+            if (walk) {
+                ra = tile_root_walk(t.uf.w, a, t.cap, d.err);
+                rb = (tb << 16) | tile_root_walk(ufb, bl, t.cap, d.err);
+            } else {
+                ra = tile_root(t.uf.w, a);
+                rb = (tb << 16) | tile_root(ufb, bl);
+            }
         }
         // A bond joining the same two tile roots with the same seam crossing
         // as the previous lane's closes a loop of winding zero (paths inside a
@@ -553,11 +558,17 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
             __syncthreads();
             cluster_union<NT>(t, tid);
             __syncthreads();
-            cluster_roots<NT>(t, tid);
-            __syncthreads();
-            cl.sync();  // every tile's roots are final
+            // With at least one word per thread the roots are found in one
+            // pass with the flip, after the boundary stage (roots_flip_pieces);
+            // the boundary bonds' tile roots are then found by read-only walks.
+            const bool merged = t.g.NW >= (uint32_t)NT;
+            if (!merged) {
+                cluster_roots<NT>(t, tid);
+                __syncthreads();
+            }
+            cl.sync();  // every tile's unions (and roots) are final
 
-            tile_boundary<NT>(x, tl, d, red.tile_end, tid);
+            tile_boundary<NT>(x, tl, d, red.tile_end, merged, tid);
             cl.sync();  // every boundary union is done
 
             // Root node of each of this tile's nodes, kept in the high half of
@@ -588,9 +599,14 @@ __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 1024 / NT)
                 }
             }
             __syncthreads();
-            // Flip run pieces by their tile root's FLIP bit; a measured sweep
-            // also leaves every piece leader's word holding its tile root.
-            flip_pieces(t, tid, NT, measure);
+            // Flip run pieces by their tile root's FLIP bit; every piece
+            // leader's word is left holding its tile root (without the merged
+            // pass only in measured sweeps), and the merged pass also sets the
+            // ROOT bits.
+            if (merged)
+                (void)roots_flip_pieces(t, tid, NT);
+            else
+                flip_pieces(t, tid, NT, measure);
             __syncthreads();
             cl.sync();  // every flip is done
             tile_halo<NT>(x, tl, cl, red, tid);

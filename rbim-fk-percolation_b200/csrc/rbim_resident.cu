@@ -327,56 +327,6 @@ __device__ __forceinline__ void phase_seam_propagate(const Res &r, uint32_t tid,
     }
 }
 
-// Roots and cluster flip of a sweep in one pass, one lane per word and one
-// walk per run piece (the sites of a word split into pieces -- maximal runs
-// of occupied y-bonds cut at the word boundary -- that share a root).  A
-// piece's leader walks read-only up to its root; the root is then written
-// into the leader's word (for a run head this is the final compression the
-// separate roots pass would make, and the count and |M_C| passes read it
-// for every leader), the piece flips as a whole with its root's FLIP bit,
-// and a leader that is its own root sets its ROOT bit.  Walks of other lanes
-// running at the same time may read a head's old parent or its final root;
-// both are ancestors, so every walk ends at the right root.  Roots' words are
-// never written.  Returns the number of roots this thread found.
-__device__ __forceinline__ uint32_t roots_flip_pieces(const Lat<Word16> &t, uint32_t tid, uint32_t nthreads)
-{
-    const Geom &g = t.g;
-    const UF<Word16> &uf = t.uf;
-    uint32_t nroots = 0;
-    for (uint32_t w = tid; w < g.NW; w += nthreads) {
-        const uint32_t valid = g.valid(w);
-        uint32_t lead = (head_mask(t.OV, w, valid) | 1u) & valid;
-        const uint32_t nv = (uint32_t)__popc(valid);
-        uint32_t fl = 0, rootbits = 0;
-        while (lead) {
-            const uint32_t b = __ffs(lead) - 1u;
-            lead &= lead - 1u;
-            const uint32_t end = lead ? (uint32_t)(__ffs(lead) - 1) : nv;
-            const uint32_t n = (w << 5) + b;
-            uint32_t x = uf.ld(n);
-            for (uint32_t it = 0;; ++it) {
-                const uint32_t p = uf.ld(x);
-                if (p == x) break;
-                if (it >= t.cap) {
-                    atomicOr(t.err, kErrFindCap);
-                    break;
-                }
-                x = p;
-            }
-            if (x == n) {
-                rootbits |= 1u << b;
-                ++nroots;
-            } else {
-                uf.st(n, (unsigned short)x);
-            }
-            if ((t.FLIP[x >> 5] >> (x & 31u)) & 1u) fl |= (end - b == 32u) ? 0xFFFFFFFFu : (((1u << (end - b)) - 1u) << b);
-        }
-        t.ROOT[w] = rootbits;
-        if (fl) t.S[w] ^= fl;
-    }
-    return nroots;
-}
-
 // The labelling stages shared by the sweep and label kernels, from occupied
 // bond planes to final roots; barriers between stages.  Returns the number of
 // roots counted by this warp.  The label kernel (sweep = false) then points

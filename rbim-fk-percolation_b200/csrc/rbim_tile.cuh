@@ -168,6 +168,22 @@ __device__ __forceinline__ unsigned long long size_key(uint32_t size, uint32_t g
     return ((unsigned long long)size << 32) | (unsigned long long)(0xFFFFFFFFu - g);
 }
 
+// Root of tile site x by a read-only walk, for use before the heads point at
+// their roots (nothing writes the parents meanwhile); at most `cap` steps,
+// after which the error bit is set and the walk's position returned.
+__device__ __forceinline__ uint32_t tile_root_walk(const unsigned short *uf, uint32_t x, uint32_t cap, int *err)
+{
+    for (uint32_t it = 0;; ++it) {
+        const uint32_t p = uf[x];
+        if (p == x) return x;
+        if (it >= cap) {
+            atomicOr(err, kErrFindCap);
+            return x;
+        }
+        x = p;
+    }
+}
+
 // Size of the tile cluster of tile root m once the sizes minus one have been
 // added onto the roots' own indices (count_pieces<true> without zeroing).
 __device__ __forceinline__ uint32_t tile_size(const unsigned short *u16, uint32_t m)
