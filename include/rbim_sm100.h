@@ -168,7 +168,7 @@ int rbim_label_wrap(int64_t L, int n_lattices, const uint8_t *occ, int32_t *labe
  * rbim_resident_max_l()).  This is the engine behind many calls of the
  * reference's run_single_realization (src/rbim/simulation.py:196-242) and
  * sw_sweep (src/rbim/swendsen_wang.py:103-172).  records may be NULL.
- * threads: CTA size, 64, 128, 256, 512 or 1024 (0 = rbim_resident_threads(l_max)).
+ * threads: CTA size, 32, 64, 128, 256, 512 or 1024 (0 = rbim_resident_threads(l_max)).
  * workspace: rbim_batched_workspace_bytes()
  * bytes (the work-queue counter).
  */

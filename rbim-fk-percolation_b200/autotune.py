@@ -33,7 +33,7 @@ __all__ = ["CANDIDATES", "size_class", "enabled", "enable", "disable", "tuned_th
            "tune_cluster", "tuned_cluster_plan"]
 
 #: CTA sizes the resident engine accepts.
-CANDIDATES = (64, 128, 256, 512, 1024)
+CANDIDATES = (32, 64, 128, 256, 512, 1024)
 
 _lock = threading.Lock()
 # "<device>|<L>" -> CTA size; "<device>|cluster|<L>" -> [CTAs per cluster, CTA size]

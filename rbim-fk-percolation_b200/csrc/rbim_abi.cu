@@ -208,8 +208,9 @@ int rbim_sweeps_batched(rbim_chain_t *chains, int n_chains, int64_t l_max, uint3
     if (!aligned16(spin_pool) || !aligned16(coupling_pool))
         return fail(RBIM_ERR_INVALID, "spin and coupling pools must be 16-byte aligned");
     if (workspace_bytes < rbim_batched_workspace_bytes()) return fail(RBIM_ERR_INVALID, "workspace too small");
-    if (threads != 0 && threads != 64 && threads != 128 && threads != 256 && threads != 512 && threads != 1024)
-        return fail(RBIM_ERR_INVALID, "threads must be 0, 64, 128, 256, 512 or 1024 (got %d)", threads);
+    if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512 &&
+        threads != 1024)
+        return fail(RBIM_ERR_INVALID, "threads must be 0, 32, 64, 128, 256, 512 or 1024 (got %d)", threads);
     cudaError_t e = rbim::launch_resident_sweeps(chains, n_chains, (int)l_max, spin_pool, coupling_pool,
                                                  (long long *)acc_int, acc_f64, records, n_sweeps, threads, 0,
                                                  (int *)workspace, status, (cudaStream_t)stream);

@@ -35,7 +35,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from . import _native, autotune
-from .engine import QUEUE_SLOT, Launch, _torch, launch_buckets, require_cuda
+from .engine import QUEUE_SLOT, Launch, _sm_count, _torch, launch_buckets, occupancy_threads, require_cuda
 from .packing import pack_couplings, threshold, words_for
 from .simulation import ScanPlan, assemble_scan, plan_temperature_scan
 
@@ -390,7 +390,9 @@ class ScanServer:
                 base = self.desc_dev.data_ptr() + 96 * first
                 if key[0] == 0:
                     nt = self.threads or autotune.tuned_threads(l_max, self.device)
-                    nt = nt or int(self.lib.rbim_resident_threads(l_max))
+                    if not nt:
+                        nt = occupancy_threads(int(self.lib.rbim_resident_threads(l_max)), count,
+                                               _sm_count(self.device))
                     on_chip.append(Launch(0, base, count, l_max, nt))
                 elif key[0] == 1:
                     plan = autotune.tuned_cluster_plan(l_max, sorted({a.plan.L for a in group}), self.device)

@@ -55,7 +55,7 @@ def test_host_only_queries(rb):
     # Default CTA size of the resident engine: a supported size, never
     # shrinking as L grows, 0 outside the engine's range.
     sizes = [lib.rbim_resident_threads(L) for L in range(3, lmax + 1)]
-    assert set(sizes) <= {64, 128, 256, 512, 1024}
+    assert set(sizes) <= {32, 64, 128, 256, 512, 1024}
     assert sizes == sorted(sizes)
     assert lib.rbim_resident_threads(2) == 0 and lib.rbim_resident_threads(lmax + 1) == 0
     # Cluster plans: CTA size 512 (half-size tiles) or 1024 wherever a cluster size exists.
@@ -118,7 +118,7 @@ def test_engine_buckets_split_modes(rb):
     r_max = nat.lib().rbim_resident_max_l()
     Ls = [16, 32, 48, 200, 300, 420, 2000]
     keys = nat.engine_buckets(Ls, r_max, 1024)
-    assert keys[0] == keys[1] == (0, 64) and keys[2] == (0, 128) and keys[3][0] == 0
+    assert keys[0] == keys[1] == (0, 32) and keys[2] == (0, 128) and keys[3][0] == 0
     assert keys[4][:2] == keys[5][:2] and keys[4] != keys[5]  # same cluster size, different CTA size
     assert keys[6] == (2, 0)
     assert max(k for k in keys if k[0] == 0) < min(k for k in keys if k[0] == 1) < (2, 0)

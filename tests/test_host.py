@@ -302,3 +302,13 @@ def test_vectorised_assembly_matches_per_temperature(rb, n_r, n_bins, measure):
         for field in ("value", "error", "thermal_error"):
             w = np.array([want[t][name][field] for t in range(len(temps))])
             np.testing.assert_allclose(got[name][field], w, rtol=1e-12, atol=1e-15, err_msg=f"{name} {field}")
+
+
+def test_occupancy_threads(rb):
+    """The resident CTA size doubles while every lattice of a launch still fits the GPU at twice the threads."""
+    occ = rb.engine.occupancy_threads
+    assert occ(32, 1280, 148) == 64  # the reference's L = 32 scan
+    assert occ(32, 524288, 148) == 32  # a full GPU keeps one-warp CTAs
+    assert occ(128, 16384, 148) == 128
+    assert occ(128, 10, 148) == 1024 and occ(1024, 1, 148) == 1024
+    assert occ(32, 2368, 148) == 64 and occ(32, 2369, 148) == 32
