@@ -33,8 +33,9 @@ __all__ = [
 class SweepResult:
     """Observables of one sweep (reference ``swendsen_wang.py:24-53``).
 
-    ``second_abs_magnetization`` is not measured by the engine (it is not a
-    primitive of the scan) and is reported as NaN.
+    Every field is measured on the device in the sweep's record, including
+    ``second_abs_magnetization`` (|M| of the second-largest cluster,
+    reference ``swendsen_wang.py:151-154``).
     """
 
     energy: float
