@@ -102,6 +102,23 @@ def test_argument_errors_are_reported_without_device_work(rb):
     assert lib.rbim_label_wrap(8, 0, None, None, None, None, None, None, 0, None) == 0
 
 
+def test_grid_workspace_covers_its_arrays(rb):
+    """Grid workspace: one 64-bit node word per site, C x L tile-root ids and a
+    flip bit per site at least, 256-byte granular, growing with L; 0 outside
+    the engine's range."""
+    lib = rb._native.lib()
+    prev = 0
+    for L in (33, 64, 100, 257, 1024, 2048, 3100):
+        for C in (2, 64, 148):
+            b = lib.rbim_grid_workspace_bytes(L, C)
+            assert b % 256 == 0 and b >= 8 * L * L + 4 * C * L + L * L // 8, (L, C)
+        cur = lib.rbim_grid_workspace_bytes(L, 148)
+        assert cur > prev, L
+        prev = cur
+    assert lib.rbim_grid_workspace_bytes(70000, 4) == 0
+    assert lib.rbim_grid_workspace_bytes(64, -1) == 0
+
+
 def test_packing_matches_the_documented_layout(rb):
     # Site n is bit n & 31 of word n >> 5; a set spin bit means s = -1.
     L = 6
